@@ -1,0 +1,182 @@
+/*
+ * s2dw_cuda.h -- C ABI of the B200 (sm_100a) implementation of the S2DW
+ * directional scale-discretised wavelet transform on the sphere.
+ *
+ * Every entry point is a plain C function over plain pointers and sizes, so
+ * that Fortran (ISO_C_BINDING), C, C++ and Python (ctypes) callers can bind
+ * it directly.  Array arguments use the reference's Fortran column-major
+ * layouts, first index fastest:
+ *
+ *   flm(0:B-1,0:B-1)                 complex128, flm[l + B*m]   (m <= l used)
+ *   K_gamma(0:J,0:B-1)               float64,    K[j + (J+1)*l]
+ *   Phi2(0:B-1)                      float64
+ *   Slm(0:B-1,0:N-1)                 complex128, S[l + B*n]
+ *   scoeff(0:bl_scoeff-1,0:bl_scoeff-1) complex128
+ *   wav(0:J,0:2B-2,0:2B-1,0:N-1)     float64, static layout, scale fastest
+ *   coeff_j(0:2bl-2,0:2bl-1,0:N-1)   float64, one array per scale j
+ *                                    (the "dynamic" layout)
+ *
+ * Return values are status codes that mirror S2DW_ERROR_* of the reference
+ * (src/mod/s2dw_error_mod.f90:37-52).  The reference prints and halts on a
+ * fatal error; this library returns the code instead and keeps a message
+ * for s2dwc_last_error_message().
+ *
+ * Host-buffer entry points are synchronous and allocate their device
+ * workspace through a per-(B,N,alpha,J,device) plan cache.  Device entry
+ * points (s2dwc_plan_*) take device pointers and a CUDA stream and never
+ * synchronise.
+ */
+#ifndef S2DW_CUDA_H
+#define S2DW_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: s2dw_error_mod.f90:37-52 */
+#define S2DWC_OK 0
+#define S2DWC_ERROR_INIT 1
+#define S2DWC_ERROR_NOT_INIT 2
+#define S2DWC_ERROR_INIT_FAIL 3
+#define S2DWC_ERROR_MEM_ALLOC_FAIL 4
+#define S2DWC_ERROR_ARTH 5
+#define S2DWC_ERROR_ARTH_WARNING 6
+#define S2DWC_ERROR_SIZE_WARNING 7
+#define S2DWC_ERROR_SIZE_INVALID 8
+#define S2DWC_ERROR_SIZE_NOT_DEF 9
+#define S2DWC_ERROR_ARG_INVALID 10
+#define S2DWC_ERROR_ARG_WARNING 11
+#define S2DWC_ERROR_QUAD_STEP_EXCEED 12
+#define S2DWC_ERROR_ADMISS_FAIL 13
+#define S2DWC_ERROR_FILEIO 14
+/* Not in the reference: a CUDA runtime call failed (device lost, launch
+ * failure).  The message names the call. */
+#define S2DWC_ERROR_CUDA 15
+
+/* Precision form of the transform. */
+#define S2DWC_FORM_FP64 0
+
+/* ---------------------------------------------------------------------- */
+/* Library state                                                          */
+/* ---------------------------------------------------------------------- */
+
+/* Version string of this library. */
+const char *s2dwc_version(void);
+
+/* Optional explicit initialisation (CUDA context on the current device).
+ * Host-buffer calls initialise lazily.  Returns S2DWC_OK. */
+int s2dwc_init(void);
+
+/* Frees every cached plan and its device memory. */
+int s2dwc_finalize(void);
+
+/* Text of a status code (the reference's error_comment table,
+ * s2dw_error_mod.f90:58-76). */
+const char *s2dwc_error_string(int code);
+
+/* Detail of the last error raised on the calling thread. */
+const char *s2dwc_last_error_message(void);
+
+/* ---------------------------------------------------------------------- */
+/* Kernel tables and helpers (host, FP64)                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces s2dw_core_assimilate_int, s2dw_core_mod.f90:1398-1415.
+ * Returns 1 (assimilated, *y set) or 0 (*y = 0). */
+int s2dwc_assimilate_int(double x, int *y);
+
+/* Replaces s2dw_core_comp_Jmax, s2dw_core_mod.f90:1365-1376. */
+int s2dwc_comp_jmax(int B, double alpha);
+
+/* Per-scale band limits bl_hi, bl_lo of scale jj, the block repeated at
+ * s2dw_core_mod.f90:372-381 / :607-616 / :850-859 / :1093-1102. */
+int s2dwc_band_limits(int jj, int B, double alpha, int *bl_hi, int *bl_lo);
+
+/* Number of doubles of scale jj's coefficient array (2bl-1)*2bl*N, the
+ * shape allocated at s2dw_core_mod.f90:746. */
+long long s2dwc_wav_scale_size(int jj, int B, int N, double alpha);
+
+/* Replaces s2dw_core_init_kernels, s2dw_core_mod.f90:97-157. */
+int s2dwc_init_kernels(double *K_gamma, double *Phi2, int *bl_scoeff, int J, int B, double alpha);
+
+/* Replaces s2dw_core_init_directionality, s2dw_core_mod.f90:219-250. */
+int s2dwc_init_directionality(double *Slm /* complex128 (B,N) */, int B, int N);
+
+/* Replaces s2dw_core_admiss, s2dw_core_mod.f90:285-304.  *pass receives
+ * 1 when every |admiss(l)-1| <= 1e-12. */
+int s2dwc_admiss(double *admiss, const double *K_gamma, const double *Phi2, int B, int J, int *pass);
+
+/* ---------------------------------------------------------------------- */
+/* Transforms on host buffers (drop-in for the Fortran entry points)      */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces s2dw_core_analysis_flm2wav, s2dw_core_mod.f90:342-534.
+ * wav: static layout (J+1, 2B-1, 2B, N); only the region a<2bl-1, b<2bl
+ * of each scale is written, as in the reference. */
+int s2dwc_analysis_flm2wav(double *wav, double *scoeff, const double *flm, const double *K_gamma,
+                           const double *Slm, int J, int B, int N, int bl_scoeff, double alpha);
+
+/* Replaces s2dw_core_analysis_flm2wav_dynamic, s2dw_core_mod.f90:572-775.
+ * wav_scales[jj] points at caller-owned storage of
+ * s2dwc_wav_scale_size(jj,...) doubles (the Fortran shim allocates
+ * wavdyn(jj)%coeff and passes c_loc of it). */
+int s2dwc_analysis_flm2wav_dynamic(double *const *wav_scales, double *scoeff, const double *flm,
+                                   const double *K_gamma, const double *Slm, int J, int B, int N,
+                                   int bl_scoeff, double alpha);
+
+/* Replaces s2dw_core_synthesis_wav2flm, s2dw_core_mod.f90:816-1019. */
+int s2dwc_synthesis_wav2flm(double *flm, const double *wav, const double *scoeff,
+                            const double *K_gamma, const double *Phi2, const double *Slm, int J,
+                            int B, int N, int bl_scoeff, double alpha);
+
+/* Replaces s2dw_core_synthesis_wav2flm_dynamic, s2dw_core_mod.f90:1060-1266.
+ * The reference frees wavdyn; here the caller keeps ownership (the Fortran
+ * shim deallocates after the call). */
+int s2dwc_synthesis_wav2flm_dynamic(double *flm, const double *const *wav_scales,
+                                    const double *scoeff, const double *K_gamma, const double *Phi2,
+                                    const double *Slm, int J, int B, int N, int bl_scoeff,
+                                    double alpha);
+
+/* ---------------------------------------------------------------------- */
+/* Device-resident API                                                    */
+/* ---------------------------------------------------------------------- */
+
+typedef struct s2dwc_plan s2dwc_plan;
+
+/* Creates a plan for (B, N, alpha, J) on CUDA device `device`: cached
+ * recurrence tables, chirp filters and workspaces.  `form` is
+ * S2DWC_FORM_FP64. */
+int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int form, int device);
+int s2dwc_plan_destroy(s2dwc_plan *plan);
+
+/* Uploads the caller's kernel tables (host pointers, reference layouts).
+ * Phi2 may be NULL for analysis-only use. */
+int s2dwc_plan_set_tables(s2dwc_plan *plan, const double *K_gamma, const double *Phi2,
+                          const double *Slm, int bl_scoeff);
+
+/* Packed per-scale wavelet layout used by the device API: scale jj starts
+ * at offsets[jj] doubles and holds coeff_j in the dynamic layout;
+ * offsets[J+1] is the total.  `offsets` has J+2 entries. */
+int s2dwc_plan_wav_offsets(const s2dwc_plan *plan, long long *offsets);
+
+/* Bytes of device workspace the plan holds. */
+long long s2dwc_plan_workspace_bytes(const s2dwc_plan *plan);
+
+/* Analysis on device memory.  d_wav: packed per-scale layout; d_scoeff:
+ * (bl_scoeff, bl_scoeff) complex; d_flm: (B, B) complex.  `stream` is a
+ * cudaStream_t (NULL = legacy default stream). */
+int s2dwc_plan_analysis(s2dwc_plan *plan, double *d_wav, double *d_scoeff, const double *d_flm,
+                        void *stream);
+
+/* Synthesis on device memory (d_flm is overwritten). */
+int s2dwc_plan_synthesis(s2dwc_plan *plan, double *d_flm, const double *d_wav,
+                         const double *d_scoeff, void *stream);
+
+/* Number of CUDA kernels one analysis / one synthesis launches. */
+int s2dwc_plan_launch_count(const s2dwc_plan *plan, int *analysis, int *synthesis);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* S2DW_CUDA_H */

@@ -1,0 +1,139 @@
+// Internal declarations shared by the host and device parts of libs2dw_cuda.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/s2dw_cuda.h"
+
+namespace s2dw {
+
+// ---------------------------------------------------------------------------
+// Errors: every failing entry point records a code and a message.
+// ---------------------------------------------------------------------------
+int set_error(int code, const char *fmt, ...);
+
+#define S2DW_CUDA_TRY(call)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return ::s2dw::set_error(S2DWC_ERROR_CUDA, "%s failed: %s (%s:%d)", #call,   \
+                                     cudaGetErrorString(e_), __FILE__, __LINE__);        \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Host helpers restating the reference's scalar routines.
+// ---------------------------------------------------------------------------
+bool assimilate_int(double x, int *y);
+int comp_jmax(int B, double alpha);
+bool params_valid(int J, int B, double alpha, int N /* <0: absent */);
+void band_limits(int jj, int B, double alpha, int *bl_hi, int *bl_lo);
+double quad_weight(double theta, int B);
+
+// Positive n set of the transform: n in [0, N) with N+n odd (the k_indicator
+// test of s2dw_core_mod.f90:693 / :1146).  Returns its size NP (<= 4 for N<=8).
+int positive_nset(int N, int *nq);
+
+// ---------------------------------------------------------------------------
+// Recurrence tables for d^l_{m'm}(pi/2), built on the host in long double.
+//   l-walk (fixed m', m, stepping l):   e_{l+1} = -a_m(l) a_m'(l) e_l - e_{l-1},
+//                                       d = Om_l(m) Om_l(m') e
+//   m'-walk (fixed l, m, stepping m' down): e_{m'-1} = m b(l,m') e_{m'} - e_{m'+1},
+//                                       d = Gam(l,m') e
+// Start values are stored as mantissa (double in [1,2)) and binary exponent.
+// All 2-D tables are [l*B + x] with zeros where x > l.
+// ---------------------------------------------------------------------------
+struct RecTables {
+    int B = 0;
+    std::vector<double> Om, Acoef;     // l-walk scale chains and coefficients
+    std::vector<double> Stm;           // l-walk start E(l0,k)/Om_l0(k) mantissa
+    std::vector<int32_t> Ste;          //   ... exponent
+    std::vector<double> Gam, Bcoef;    // m'-walk chains and coefficients
+    std::vector<double> Em;            // edge values E(l,m)=sqrt(C(2l,l+m))/2^l
+    std::vector<int32_t> Ee;
+    std::vector<double> H;             // d^l_{m'n}(pi/2), n<8: [(l*8+n)*B + m']
+};
+void build_rec_tables(int B, RecTables &t);
+
+// ---------------------------------------------------------------------------
+// Chirp-z (Bluestein) transform specification:
+//   y[b] = sum_{k<K} x[k] exp(2 pi i s (k+k0)(b+b0)/L),  b < Bout,
+// with k0, b0 integers or half-integers (passed doubled).
+// ---------------------------------------------------------------------------
+struct CztSpec {
+    int K, Bout, L, s, k0x2, b0x2, M;
+};
+int czt_size(int K, int Bout);  // power of two M >= max(16, K+Bout-1)
+void build_czt_tables(const CztSpec &c, std::vector<double2> &pre, std::vector<double2> &post,
+                      std::vector<double2> &Hf);
+// Two-level twiddle tables for a power-of-two FFT of size M:
+// W_M^x = hi[x >> 6] * lo[x & 63], W_M = exp(-2 pi i / M).
+void build_twiddles(int M, std::vector<double2> &hi, std::vector<double2> &lo);
+
+// ---------------------------------------------------------------------------
+// Device kernels (s2dw_kernels.cu)
+// ---------------------------------------------------------------------------
+enum CztMode { CZT_ANA_BETA = 0, CZT_ANA_ALPHA = 1, CZT_SYN_ALPHA = 2, CZT_SYN_BETA = 3 };
+
+struct CztDev {
+    int M = 0;
+    CztSpec spec{};
+    double2 *pre = nullptr, *post = nullptr, *Hf = nullptr;
+};
+
+struct TwDev {
+    int M = 0;
+    double2 *hi = nullptr, *lo = nullptr;
+};
+
+struct LwalkArgs {
+    int B, N, NP, bl, blo;
+    int nq[4];
+    const double *Om, *Acoef, *Stm;
+    const int32_t *Ste;
+    const double *H;
+    const double *kappa;  // [l*NP + q] for this scale
+    const double2 *flm;   // (B,B) column-major
+    double2 *Tg;          // [g][m][m'] N x bl x bl
+};
+
+struct MwalkArgs {
+    int B, N, NP, bl, blo;
+    int nq[4];
+    const double *Gam, *Bcoef, *Em;
+    const int32_t *Ee;
+    const double *H;
+    const double *kappa;  // [l*NP + q] for this scale
+    const double2 *V2f;   // [q][m][m'] NP x bl x bl
+    double2 *flm;         // (B,B) column-major, accumulated
+};
+
+struct CztArgs {
+    int mode, bl, N, NP, rows;
+    int nq[4];
+    CztDev czt;
+    TwDev tw;
+    const double2 *in_c;   // complex input (Tg, Tb, V)
+    const double *in_r;    // real input (wavelet coefficients)
+    double2 *out_c;        // complex output (Tb, V, V2f)
+    double *out_r;         // real output (wavelet coefficients)
+    const double *wq;      // quadrature weights (2bl) for CZT_SYN_BETA
+    double scale;          // (4 pi^2/N)/(2bl-1) for CZT_SYN_ALPHA
+};
+
+int launch_lwalk(const LwalkArgs &a, cudaStream_t s);
+int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
+int launch_czt(const CztArgs &a, cudaStream_t s);
+int launch_zero(double *p, long long n, cudaStream_t s);
+int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
+int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,
+                       cudaStream_t s);
+int launch_static_scatter(double *wav_static, const double *wav_packed, int J, int B, int N,
+                          int jj, int bl, long long off, cudaStream_t s);
+int launch_static_gather(double *wav_packed, const double *wav_static, int J, int B, int N, int jj,
+                         int bl, long long off, cudaStream_t s);
+
+}  // namespace s2dw

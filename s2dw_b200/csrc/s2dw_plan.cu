@@ -1,0 +1,638 @@
+// Plans, the plan cache and the C-ABI transform entry points.
+//
+// A plan holds everything that depends only on (B, N, alpha, J, device):
+// the recurrence tables for d^l(pi/2), the chirp-z tables of every scale and
+// the device workspaces.  The caller's kernel tables (K_gamma, Phi2, Slm) are
+// uploaded per call (s2dwc_plan_set_tables), which folds them into per-scale
+// factors kappa(j,l,n).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "s2dw_internal.h"
+
+using namespace s2dw;
+
+struct s2dwc_plan {
+    int B = 0, N = 0, J = 0, device = 0, form = 0, NP = 0;
+    double alpha = 0.0;
+    int nq[4] = {0, 0, 0, 0};
+    int bl_scoeff = 0;
+    bool tables_set = false;
+    std::vector<int> bl, blo;
+    std::vector<long long> wav_off;  // J+2 entries
+    // recurrence tables
+    double *Om = nullptr, *Acoef = nullptr, *Stm = nullptr, *Gam = nullptr, *Bcoef = nullptr,
+           *Em = nullptr, *H = nullptr;
+    int32_t *Ste = nullptr, *Ee = nullptr;
+    // per-scale chirp-z tables: [scale][mode]
+    std::vector<std::array<CztDev, 4>> czt;
+    std::map<int, TwDev> tw;
+    std::vector<double *> wq;  // quadrature weights per scale
+    // caller tables
+    double *kappaA = nullptr, *kappaS = nullptr, *Phi2 = nullptr;
+    // workspaces
+    double2 *wsA = nullptr, *wsC = nullptr;
+    // device buffers of the host-buffer entry points (allocated on first use)
+    double *hbWav = nullptr;
+    double2 *hbFlm = nullptr, *hbSc = nullptr;
+    int hbSc_n = 0;
+    long long ws_bytes = 0;
+    std::vector<void *> allocs;
+    std::mutex mu;  // serialises use of the workspaces
+
+    ~s2dwc_plan()
+    {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        for (void *p : allocs) cudaFree(p);
+        cudaSetDevice(cur);
+    }
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(s2dwc_plan *p, T **ptr, size_t count)
+{
+    void *v = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&v, count * sizeof(T));
+    if (e != cudaSuccess)
+        return set_error(S2DWC_ERROR_MEM_ALLOC_FAIL, "cudaMalloc of %zu bytes failed: %s",
+                         count * sizeof(T), cudaGetErrorString(e));
+    p->allocs.push_back(v);
+    p->ws_bytes += (long long)(count * sizeof(T));
+    *ptr = static_cast<T *>(v);
+    return S2DWC_OK;
+}
+
+template <typename T>
+int dev_upload(s2dwc_plan *p, T **ptr, const std::vector<T> &h)
+{
+    int st = dev_alloc(p, ptr, h.size());
+    if (st) return st;
+    S2DW_CUDA_TRY(cudaMemcpy(*ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return S2DWC_OK;
+}
+
+int plan_build(s2dwc_plan *p)
+{
+    const int B = p->B, N = p->N, J = p->J;
+    p->NP = positive_nset(N, p->nq);
+    p->bl.resize(J + 1);
+    p->blo.resize(J + 1);
+    p->wav_off.assign(J + 2, 0);
+    for (int j = 0; j <= J; j++) {
+        band_limits(j, B, p->alpha, &p->bl[j], &p->blo[j]);
+        p->wav_off[j + 1] = p->wav_off[j] + (long long)(2 * p->bl[j] - 1) * (2 * p->bl[j]) * N;
+    }
+    RecTables t;
+    build_rec_tables(B, t);
+    int st;
+    if ((st = dev_upload(p, &p->Om, t.Om)) || (st = dev_upload(p, &p->Acoef, t.Acoef)) ||
+        (st = dev_upload(p, &p->Stm, t.Stm)) || (st = dev_upload(p, &p->Ste, t.Ste)) ||
+        (st = dev_upload(p, &p->Gam, t.Gam)) || (st = dev_upload(p, &p->Bcoef, t.Bcoef)) ||
+        (st = dev_upload(p, &p->Em, t.Em)) || (st = dev_upload(p, &p->Ee, t.Ee)) ||
+        (st = dev_upload(p, &p->H, t.H)))
+        return st;
+
+    // chirp-z tables per scale and mode
+    p->czt.resize(J + 1);
+    p->wq.resize(J + 1);
+    std::map<int, std::array<CztDev, 4>> by_bl;
+    std::map<int, double *> wq_by_bl;
+    for (int j = 0; j <= J; j++) {
+        const int b = p->bl[j], n = 2 * b - 1;
+        auto it = by_bl.find(b);
+        if (it == by_bl.end()) {
+            std::array<CztDev, 4> arr;
+            CztSpec specs[4] = {
+                {2 * b - 1, 2 * b, 4 * b, +1, -2 * (b - 1), 1, 0},  // CZT_ANA_BETA
+                {n, n, n, +1, 0, 0, 0},                              // CZT_ANA_ALPHA
+                {n, n, n, -1, 0, 0, 0},                              // CZT_SYN_ALPHA
+                {2 * b, 2 * b - 1, 4 * b, -1, 1, -2 * (b - 1), 0},  // CZT_SYN_BETA
+            };
+            for (int md = 0; md < 4; md++) {
+                CztSpec c = specs[md];
+                c.M = czt_size(c.K, c.Bout);
+                std::vector<double2> pre, post, Hf;
+                build_czt_tables(c, pre, post, Hf);
+                CztDev d;
+                d.M = c.M;
+                d.spec = c;
+                if ((st = dev_upload(p, &d.pre, pre)) || (st = dev_upload(p, &d.post, post)) ||
+                    (st = dev_upload(p, &d.Hf, Hf)))
+                    return st;
+                arr[md] = d;
+                if (!p->tw.count(c.M)) {
+                    std::vector<double2> hi, lo;
+                    build_twiddles(c.M, hi, lo);
+                    TwDev tw;
+                    tw.M = c.M;
+                    if ((st = dev_upload(p, &tw.hi, hi)) || (st = dev_upload(p, &tw.lo, lo))) return st;
+                    p->tw[c.M] = tw;
+                }
+            }
+            it = by_bl.emplace(b, arr).first;
+            std::vector<double> w(2 * b);
+            for (int bb = 0; bb < 2 * b; bb++)
+                w[bb] = quad_weight(M_PI * (2.0 * bb + 1.0) / (4.0 * b), b);
+            double *dw;
+            if ((st = dev_upload(p, &dw, w))) return st;
+            wq_by_bl[b] = dw;
+        }
+        p->czt[j] = it->second;
+        p->wq[j] = wq_by_bl[b];
+    }
+    // kernel-table factors
+    if ((st = dev_alloc(p, &p->kappaA, (size_t)(J + 1) * B * p->NP)) ||
+        (st = dev_alloc(p, &p->kappaS, (size_t)(J + 1) * B * p->NP)) ||
+        (st = dev_alloc(p, &p->Phi2, (size_t)B)))
+        return st;
+    // workspaces: wsA holds Tb / V (N x bl x 2bl), wsC holds Tg / V2f
+    const size_t nA = (size_t)N * B * 2 * B, nC = (size_t)std::max(N, p->NP) * B * B;
+    if ((st = dev_alloc(p, &p->wsA, nA)) || (st = dev_alloc(p, &p->wsC, nC))) return st;
+    return S2DWC_OK;
+}
+
+std::mutex g_cache_mu;
+std::map<std::tuple<int, int, int, int, long long, int>, std::unique_ptr<s2dwc_plan>> g_cache;
+
+int validate_sizes(int B, int N, double alpha, int J)
+{
+    if (B < 2) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d must be >= 2", B);
+    if (N < 1 || N > 8)
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d unsupported (1 <= N <= 8)", N);
+    if (N > B) return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d exceeds B=%d", N, B);
+    if (!(alpha > 1.0)) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha=%g must exceed 1", alpha);
+    if (B > 2048) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d exceeds the supported 2048", B);
+    if (!params_valid(J, B, alpha, N))
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d invalid for B=%d alpha=%g (1<=J<=%d)", J, B,
+                         alpha, comp_jmax(B, alpha));
+    return S2DWC_OK;
+}
+
+int get_cached_plan(int B, int N, double alpha, int J, s2dwc_plan **out)
+{
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    long long abits;
+    std::memcpy(&abits, &alpha, sizeof(abits));
+    auto key = std::make_tuple(B, N, J, dev, abits, 0);
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) {
+        *out = it->second.get();
+        return S2DWC_OK;
+    }
+    s2dwc_plan *p = nullptr;
+    int st = s2dwc_plan_create(&p, B, N, alpha, J, S2DWC_FORM_FP64, dev);
+    if (st) return st;
+    g_cache.emplace(key, std::unique_ptr<s2dwc_plan>(p));
+    *out = p;
+    return S2DWC_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Runs the analysis of every scale on `s`.
+int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s)
+{
+    int st;
+    for (int j = 0; j <= p->J; j++) {
+        const int bl = p->bl[j];
+        LwalkArgs la{};
+        la.B = p->B;
+        la.N = p->N;
+        la.NP = p->NP;
+        la.bl = bl;
+        la.blo = p->blo[j];
+        std::memcpy(la.nq, p->nq, sizeof(la.nq));
+        la.Om = p->Om;
+        la.Acoef = p->Acoef;
+        la.Stm = p->Stm;
+        la.Ste = p->Ste;
+        la.H = p->H;
+        la.kappa = p->kappaA + (size_t)j * p->B * p->NP;
+        la.flm = d_flm;
+        la.Tg = p->wsC;
+        if ((st = launch_lwalk(la, s))) return st;
+
+        CztArgs ca{};
+        ca.mode = CZT_ANA_BETA;
+        ca.bl = bl;
+        ca.N = p->N;
+        ca.NP = p->NP;
+        std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
+        ca.rows = p->N * bl;
+        ca.czt = p->czt[j][CZT_ANA_BETA];
+        ca.tw = p->tw[ca.czt.M];
+        ca.in_c = p->wsC;
+        ca.out_c = p->wsA;
+        if ((st = launch_czt(ca, s))) return st;
+
+        ca.mode = CZT_ANA_ALPHA;
+        ca.rows = p->N * bl;  // (g, b pair)
+        ca.czt = p->czt[j][CZT_ANA_ALPHA];
+        ca.tw = p->tw[ca.czt.M];
+        ca.in_c = p->wsA;
+        ca.out_c = nullptr;
+        ca.out_r = d_wav + p->wav_off[j];
+        if ((st = launch_czt(ca, s))) return st;
+    }
+    return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
+}
+
+int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const double2 *d_scoeff,
+                  cudaStream_t s)
+{
+    int st;
+    if ((st = launch_zero(reinterpret_cast<double *>(d_flm), 2LL * p->B * p->B, s))) return st;
+    for (int j = 0; j <= p->J; j++) {
+        const int bl = p->bl[j];
+        CztArgs ca{};
+        ca.mode = CZT_SYN_ALPHA;
+        ca.bl = bl;
+        ca.N = p->N;
+        ca.NP = p->NP;
+        std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
+        ca.rows = p->N * bl;
+        ca.czt = p->czt[j][CZT_SYN_ALPHA];
+        ca.tw = p->tw[ca.czt.M];
+        ca.in_r = d_wav + p->wav_off[j];
+        ca.out_c = p->wsA;
+        ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
+        if ((st = launch_czt(ca, s))) return st;
+
+        ca.mode = CZT_SYN_BETA;
+        ca.rows = p->NP * bl;
+        ca.czt = p->czt[j][CZT_SYN_BETA];
+        ca.tw = p->tw[ca.czt.M];
+        ca.in_c = p->wsA;
+        ca.in_r = nullptr;
+        ca.out_c = p->wsC;
+        ca.wq = p->wq[j];
+        if ((st = launch_czt(ca, s))) return st;
+
+        MwalkArgs ma{};
+        ma.B = p->B;
+        ma.N = p->N;
+        ma.NP = p->NP;
+        ma.bl = bl;
+        ma.blo = p->blo[j];
+        std::memcpy(ma.nq, p->nq, sizeof(ma.nq));
+        ma.Gam = p->Gam;
+        ma.Bcoef = p->Bcoef;
+        ma.Em = p->Em;
+        ma.Ee = p->Ee;
+        ma.H = p->H;
+        ma.kappa = p->kappaS + (size_t)j * p->B * p->NP;
+        ma.V2f = p->wsC;
+        ma.flm = d_flm;
+        if ((st = launch_mwalk(ma, s))) return st;
+    }
+    return launch_scaling_add(d_flm, d_scoeff, p->Phi2, p->B, p->bl_scoeff, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *s2dwc_version(void) { return "s2dw-b200 0.1 (sm_100a, FP64)"; }
+
+int s2dwc_init(void)
+{
+    S2DW_CUDA_TRY(cudaFree(nullptr));
+    return S2DWC_OK;
+}
+
+int s2dwc_finalize(void)
+{
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    g_cache.clear();
+    return S2DWC_OK;
+}
+
+const char *s2dwc_error_string(int code)
+{
+    static const char *txt[] = {
+        "No error",
+        "Attempt to initialise object that has already been initialised",
+        "Object not initialised",
+        "Object initialisation failed",
+        "Memory allocation failed",
+        "Arithmetic exception",
+        "Arithmetic warning",
+        "Warning: Sizes not in recommended range",
+        "Invalid sizes",
+        "Sizes not defined",
+        "Arguments invalid",
+        "Argument warning",
+        "Exceeded number of steps limit whem computing quadrature",
+        "Admissibility test failed (resolution of identity not satisfied)",
+        "File IO error",
+        "CUDA runtime error",
+    };
+    if (code < 0 || code > 15) return "Unknown error";
+    return txt[code];
+}
+
+int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int form, int device)
+{
+    if (!plan) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_create: null output");
+    *plan = nullptr;
+    int st = validate_sizes(B, N, alpha, J);
+    if (st) return st;
+    if (form != S2DWC_FORM_FP64) return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
+    int ndev = 0;
+    S2DW_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev)
+        return set_error(S2DWC_ERROR_ARG_INVALID, "device %d out of range (%d devices)", device, ndev);
+    DeviceGuard dg(device);
+    auto *p = new s2dwc_plan();
+    p->B = B;
+    p->N = N;
+    p->J = J;
+    p->alpha = alpha;
+    p->form = form;
+    p->device = device;
+    st = plan_build(p);
+    if (st) {
+        delete p;
+        return st;
+    }
+    *plan = p;
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_destroy(s2dwc_plan *plan)
+{
+    delete plan;
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Phi2, const double *Slm_,
+                          int bl_scoeff)
+{
+    if (!p || !K_gamma || !Slm_) return set_error(S2DWC_ERROR_ARG_INVALID, "set_tables: null pointer");
+    const int B = p->B, N = p->N, J = p->J, NP = p->NP;
+    if (bl_scoeff < 0 || bl_scoeff > B)
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "bl_scoeff=%d outside [0,B]", bl_scoeff);
+    const std::complex<double> *S = reinterpret_cast<const std::complex<double> *>(Slm_);
+    // The kernels factor S(l,n) = s(l,n) * eta with eta = 1 (N odd) or i
+    // (N even), the form s2dw_core_init_directionality produces
+    // (s2dw_core_mod.f90:240-245).  Entries with N+n even are never used.
+    const bool even = (N % 2 == 0);
+    std::vector<double> s((size_t)B * NP);
+    for (int q = 0; q < NP; q++)
+        for (int l = 0; l < B; l++) {
+            std::complex<double> v = S[l + (size_t)B * p->nq[q]];
+            double other = even ? v.real() : v.imag();
+            if (other != 0.0)
+                return set_error(S2DWC_ERROR_ARG_INVALID,
+                                 "Slm(%d,%d) is not of the form s*%s produced by init_directionality",
+                                 l, p->nq[q], even ? "i" : "1");
+            s[(size_t)l * NP + q] = even ? v.imag() : v.real();
+        }
+    std::vector<double> kA((size_t)(J + 1) * B * NP), kS((size_t)(J + 1) * B * NP);
+    const double c8 = 8.0 * (M_PI * M_PI);
+    for (int j = 0; j <= J; j++)
+        for (int l = 0; l < B; l++) {
+            const double K = K_gamma[j + (size_t)(J + 1) * l];
+            for (int q = 0; q < NP; q++) {
+                const int n = p->nq[q];
+                const double sv = s[(size_t)l * NP + q];
+                kA[((size_t)j * B + l) * NP + q] = K * sv;
+                // (2l+1)/(8 pi^2) (1 or 2) K S i^{-n} with the eta i^{-n}
+                // phase reduced to the real sign (-1)^floor(n/2)
+                const double sig = ((n / 2) & 1) ? -1.0 : 1.0;
+                kS[((size_t)j * B + l) * NP + q] =
+                    ((double)(2 * l + 1) / c8) * (n == 0 ? 1.0 : 2.0) * K * sv * sig;
+            }
+        }
+    DeviceGuard dg(p->device);
+    S2DW_CUDA_TRY(cudaMemcpy(p->kappaA, kA.data(), kA.size() * sizeof(double), cudaMemcpyHostToDevice));
+    S2DW_CUDA_TRY(cudaMemcpy(p->kappaS, kS.data(), kS.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (Phi2)
+        S2DW_CUDA_TRY(cudaMemcpy(p->Phi2, Phi2, (size_t)B * sizeof(double), cudaMemcpyHostToDevice));
+    else
+        S2DW_CUDA_TRY(cudaMemset(p->Phi2, 0, (size_t)B * sizeof(double)));
+    p->bl_scoeff = bl_scoeff;
+    p->tables_set = true;
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_wav_offsets(const s2dwc_plan *p, long long *offsets)
+{
+    if (!p || !offsets) return set_error(S2DWC_ERROR_ARG_INVALID, "wav_offsets: null pointer");
+    for (int j = 0; j <= p->J + 1; j++) offsets[j] = p->wav_off[j];
+    return S2DWC_OK;
+}
+
+long long s2dwc_plan_workspace_bytes(const s2dwc_plan *p) { return p ? p->ws_bytes : 0; }
+
+int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
+{
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "launch_count: null plan");
+    if (analysis) *analysis = 3 * (p->J + 1) + 1;
+    int ns = 2;
+    for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? 1 : 0);
+    if (synthesis) *synthesis = ns;
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_analysis(s2dwc_plan *p, double *d_wav, double *d_scoeff, const double *d_flm, void *stream)
+{
+    if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis: null pointer");
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis: tables not set");
+    DeviceGuard dg(p->device);
+    return run_analysis(p, d_wav, reinterpret_cast<double2 *>(d_scoeff),
+                        reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
+}
+
+int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, const double *d_scoeff, void *stream)
+{
+    if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis: null pointer");
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis: tables not set");
+    DeviceGuard dg(p->device);
+    return run_synthesis(p, reinterpret_cast<double2 *>(d_flm), d_wav,
+                         reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// Host-buffer entry points
+// ---------------------------------------------------------------------------
+
+// Device buffers of the host-buffer entry points, owned by the plan and
+// reused across calls (the plan mutex serialises their use).
+struct HostCallBuffers {
+    double *wav = nullptr;
+    double2 *flm = nullptr, *sc = nullptr;
+};
+
+static int host_prepare(int B, int N, double alpha, int J, int bl_scoeff, const double *K_gamma,
+                        const double *Phi2, const double *Slm, s2dwc_plan **pp, HostCallBuffers &hb)
+{
+    int st = validate_sizes(B, N, alpha, J);
+    if (st) return st;
+    if ((st = get_cached_plan(B, N, alpha, J, pp))) return st;
+    s2dwc_plan *p = *pp;
+    if ((st = s2dwc_plan_set_tables(p, K_gamma, Phi2, Slm, bl_scoeff))) return st;
+    DeviceGuard dg(p->device);
+    if (!p->hbWav) {
+        if ((st = dev_alloc(p, &p->hbWav, (size_t)std::max(1LL, p->wav_off[J + 1]))) ||
+            (st = dev_alloc(p, &p->hbFlm, (size_t)B * B)))
+            return st;
+    }
+    if (p->hbSc_n < bl_scoeff * bl_scoeff || !p->hbSc) {
+        if ((st = dev_alloc(p, &p->hbSc, (size_t)std::max(1, bl_scoeff * bl_scoeff)))) return st;
+        p->hbSc_n = std::max(1, bl_scoeff * bl_scoeff);
+    }
+    hb.wav = p->hbWav;
+    hb.flm = p->hbFlm;
+    hb.sc = p->hbSc;
+    return S2DWC_OK;
+}
+
+static int analysis_host(double *wav_static, double *const *wav_scales, double *scoeff, const double *flm,
+                         const double *K_gamma, const double *Slm, int J, int B, int N, int bl_scoeff,
+                         double alpha)
+{
+    if (!flm || !K_gamma || !Slm || (!scoeff && bl_scoeff > 0) || (!wav_static && !wav_scales))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null pointer");
+    s2dwc_plan *p = nullptr;
+    HostCallBuffers hb;
+    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, nullptr, Slm, &p, hb);
+    if (st) return st;
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard dg(p->device);
+    S2DW_CUDA_TRY(cudaMemcpy(hb.flm, flm, sizeof(double2) * (size_t)B * B, cudaMemcpyHostToDevice));
+    if ((st = run_analysis(p, hb.wav, hb.sc, hb.flm, 0))) return st;
+    if (bl_scoeff > 0)
+        S2DW_CUDA_TRY(cudaMemcpy(scoeff, hb.sc, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
+                                 cudaMemcpyDeviceToHost));
+    if (wav_scales) {
+        for (int j = 0; j <= J; j++)
+            S2DW_CUDA_TRY(cudaMemcpy(wav_scales[j], hb.wav + p->wav_off[j],
+                                     sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
+                                     cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<double> tmp((size_t)p->wav_off[J + 1]);
+        S2DW_CUDA_TRY(cudaMemcpy(tmp.data(), hb.wav, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost));
+        // scatter into wav(0:J,0:2B-2,0:2B-1,0:N-1); untouched outside each
+        // scale's region, as in s2dw_core_mod.f90:509
+        const size_t J1 = (size_t)J + 1, A = 2 * (size_t)B - 1, BB = 2 * (size_t)B;
+        for (int j = 0; j <= J; j++) {
+            const int bl = p->bl[j], n = 2 * bl - 1;
+            const double *src = tmp.data() + p->wav_off[j];
+#pragma omp parallel for collapse(2)
+            for (int g = 0; g < N; g++)
+                for (int b = 0; b < 2 * bl; b++)
+                    for (int a = 0; a < n; a++)
+                        wav_static[j + J1 * (a + A * (b + BB * g))] = src[a + (size_t)n * (b + 2 * (size_t)bl * g)];
+        }
+    }
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int s2dwc_analysis_flm2wav(double *wav, double *scoeff, const double *flm, const double *K_gamma,
+                           const double *Slm, int J, int B, int N, int bl_scoeff, double alpha)
+{
+    if (!wav) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null wav");
+    return analysis_host(wav, nullptr, scoeff, flm, K_gamma, Slm, J, B, N, bl_scoeff, alpha);
+}
+
+int s2dwc_analysis_flm2wav_dynamic(double *const *wav_scales, double *scoeff, const double *flm,
+                                   const double *K_gamma, const double *Slm, int J, int B, int N,
+                                   int bl_scoeff, double alpha)
+{
+    if (!wav_scales) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null wav_scales");
+    for (int j = 0; j <= J; j++)
+        if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: wav_scales[%d] is null", j);
+    return analysis_host(nullptr, wav_scales, scoeff, flm, K_gamma, Slm, J, B, N, bl_scoeff, alpha);
+}
+
+static int synthesis_host(double *flm, const double *wav_static, const double *const *wav_scales,
+                          const double *scoeff, const double *K_gamma, const double *Phi2,
+                          const double *Slm, int J, int B, int N, int bl_scoeff, double alpha)
+{
+    if (!flm || !K_gamma || !Phi2 || !Slm || (!scoeff && bl_scoeff > 0) || (!wav_static && !wav_scales))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null pointer");
+    s2dwc_plan *p = nullptr;
+    HostCallBuffers hb;
+    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, Phi2, Slm, &p, hb);
+    if (st) return st;
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard dg(p->device);
+    if (wav_scales) {
+        for (int j = 0; j <= J; j++)
+            S2DW_CUDA_TRY(cudaMemcpy(hb.wav + p->wav_off[j], wav_scales[j],
+                                     sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
+                                     cudaMemcpyHostToDevice));
+    } else {
+        std::vector<double> tmp((size_t)p->wav_off[J + 1]);
+        const size_t J1 = (size_t)J + 1, A = 2 * (size_t)B - 1, BB = 2 * (size_t)B;
+        for (int j = 0; j <= J; j++) {
+            const int bl = p->bl[j], n = 2 * bl - 1;
+            double *dst = tmp.data() + p->wav_off[j];
+#pragma omp parallel for collapse(2)
+            for (int g = 0; g < N; g++)
+                for (int b = 0; b < 2 * bl; b++)
+                    for (int a = 0; a < n; a++)
+                        dst[a + (size_t)n * (b + 2 * (size_t)bl * g)] = wav_static[j + J1 * (a + A * (b + BB * g))];
+        }
+        S2DW_CUDA_TRY(cudaMemcpy(hb.wav, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice));
+    }
+    if (bl_scoeff > 0)
+        S2DW_CUDA_TRY(cudaMemcpy(hb.sc, scoeff, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
+                                 cudaMemcpyHostToDevice));
+    if ((st = run_synthesis(p, hb.flm, hb.wav, hb.sc, 0))) return st;
+    S2DW_CUDA_TRY(cudaMemcpy(flm, hb.flm, sizeof(double2) * (size_t)B * B, cudaMemcpyDeviceToHost));
+    return S2DWC_OK;
+}
+
+int s2dwc_synthesis_wav2flm(double *flm, const double *wav, const double *scoeff, const double *K_gamma,
+                            const double *Phi2, const double *Slm, int J, int B, int N, int bl_scoeff,
+                            double alpha)
+{
+    if (!wav) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null wav");
+    return synthesis_host(flm, wav, nullptr, scoeff, K_gamma, Phi2, Slm, J, B, N, bl_scoeff, alpha);
+}
+
+int s2dwc_synthesis_wav2flm_dynamic(double *flm, const double *const *wav_scales, const double *scoeff,
+                                    const double *K_gamma, const double *Phi2, const double *Slm, int J,
+                                    int B, int N, int bl_scoeff, double alpha)
+{
+    if (!wav_scales) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null wav_scales");
+    for (int j = 0; j <= J; j++)
+        if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: wav_scales[%d] is null", j);
+    return synthesis_host(flm, nullptr, wav_scales, scoeff, K_gamma, Phi2, Slm, J, B, N, bl_scoeff, alpha);
+}
+
+}  // extern "C"
+

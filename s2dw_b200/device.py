@@ -1,0 +1,103 @@
+"""Device-resident API: a plan for (B, N, alpha, J) and transforms on CUDA
+tensors (torch is used only to own device memory and streams).
+
+Layouts on the device (all contiguous):
+  flm     complex128, B*B values, flm[l + B*m]          (torch shape (B, B) = flm^T)
+  scoeff  complex128, bs*bs values, scoeff[l + bs*m]
+  wav     float64, packed per-scale layout; scale jj occupies
+          [offsets[jj], offsets[jj+1]) in coeff(a, b, g) order (a fastest).
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import check, lib
+from .core import band_limits
+
+
+class Plan:
+    def __init__(self, B, N, alpha, J, device=0):
+        import torch
+
+        self.B, self.N, self.alpha, self.J, self.device = int(B), int(N), float(alpha), int(J), int(device)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(lib().s2dwc_plan_create(ctypes.byref(h), self.B, self.N, self.alpha, self.J, 0, self.device))
+        self._h = h
+        offs = (ctypes.c_longlong * (J + 2))()
+        check(lib().s2dwc_plan_wav_offsets(self._h, offs))
+        self.wav_offsets = [int(v) for v in offs]
+        self.bl = [band_limits(j, B, alpha)[0] for j in range(J + 1)]
+        self.bl_scoeff = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().s2dwc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def wav_size(self):
+        return self.wav_offsets[-1]
+
+    def workspace_bytes(self):
+        return int(lib().s2dwc_plan_workspace_bytes(self._h))
+
+    def launch_counts(self):
+        a, s = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().s2dwc_plan_launch_count(self._h, ctypes.byref(a), ctypes.byref(s)))
+        return a.value, s.value
+
+    def set_tables(self, K_gamma, Phi2, Slm, bl_scoeff):
+        dp = ctypes.POINTER(ctypes.c_double)
+        K = np.asfortranarray(K_gamma, dtype=np.float64)
+        S = np.asfortranarray(Slm, dtype=np.complex128)
+        P = None if Phi2 is None else np.ascontiguousarray(Phi2, dtype=np.float64)
+        check(lib().s2dwc_plan_set_tables(self._h, K.ctypes.data_as(dp),
+                                          None if P is None else P.ctypes.data_as(dp),
+                                          S.ctypes.data_as(dp), int(bl_scoeff)))
+        self.bl_scoeff = int(bl_scoeff)
+
+    def scale_view(self, wav, jj):
+        """View of scale jj of a packed wav tensor as (N, 2bl, 2bl-1) in C
+        order, i.e. coeff(a, b, g) at [g, b, a]."""
+        b = self.bl[jj]
+        return wav[self.wav_offsets[jj]:self.wav_offsets[jj + 1]].view(self.N, 2 * b, 2 * b - 1)
+
+    @staticmethod
+    def _ptr(t, dtype, numel):
+        import torch
+
+        if t is None:
+            return None
+        if not t.is_cuda or not t.is_contiguous() or t.dtype != dtype or t.numel() < numel:
+            raise ValueError(f"expected a contiguous CUDA {dtype} tensor of >= {numel} elements")
+        return ctypes.c_void_p(t.data_ptr())
+
+    @staticmethod
+    def _stream(stream):
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream()
+        return ctypes.c_void_p(s.cuda_stream)
+
+    def analysis(self, flm, wav, scoeff, stream=None):
+        import torch
+
+        check(lib().s2dwc_plan_analysis(self._h, self._ptr(wav, torch.float64, self.wav_size),
+                                        self._ptr(scoeff, torch.complex128, self.bl_scoeff ** 2),
+                                        self._ptr(flm, torch.complex128, self.B * self.B),
+                                        self._stream(stream)))
+
+    def synthesis(self, wav, scoeff, flm, stream=None):
+        import torch
+
+        check(lib().s2dwc_plan_synthesis(self._h, self._ptr(flm, torch.complex128, self.B * self.B),
+                                         self._ptr(wav, torch.float64, self.wav_size),
+                                         self._ptr(scoeff, torch.complex128, self.bl_scoeff ** 2),
+                                         self._stream(stream)))

@@ -1,0 +1,45 @@
+"""Seeded synthetic inputs with the shapes and statistics of the benchmark
+workloads (no public dataset is involved).
+
+gaussian_flm: harmonic coefficients of a real signal with angular power
+spectrum C_l = (1/(l(l+1)))^power for l >= 2 and f_00 = f_1m = 0.  Only m >= 0
+is stored (flm(l, m), l fastest, entries with m > l are zero), the layout of
+the reference's flm(0:B-1, 0:B-1).  f_l0 ~ N(0, C_l) is real; for m > 0 the
+real and imaginary parts are each N(0, C_l/2).  Draws come from numpy's
+PCG64 Generator seeded with `seed`, in l-major order, then m, real part before
+imaginary part, one standard-normal stream for the whole array.
+"""
+import numpy as np
+
+
+def gaussian_flm(B, seed=0, power=1.0):
+    rng = np.random.default_rng(seed)
+    flm = np.zeros((B, B), dtype=np.complex128, order="F")
+    if B <= 2:
+        return flm
+    ls = np.arange(2, B)
+    counts = 2 * ls + 1  # re(l,0), then (re, im) for m = 1..l
+    z = rng.standard_normal(int(counts.sum()))
+    pos = 0
+    for l in ls:
+        cl = (1.0 / (l * (l + 1.0))) ** power
+        s = np.sqrt(cl)
+        h = np.sqrt(cl / 2.0)
+        flm[l, 0] = z[pos] * s
+        re = z[pos + 1:pos + 2 * l + 1:2]
+        im = z[pos + 2:pos + 2 * l + 1:2]
+        flm[l, 1:l + 1] = h * (re + 1j * im)
+        pos += 2 * l + 1
+    return flm
+
+
+def transform_setup(B, N, alpha=2.0, J=None):
+    """Kernel tables of the library for (B, N, alpha, J=Jmax by default):
+    returns dict with J, K_gamma, Phi2, bl_scoeff, Slm."""
+    from . import core
+
+    if J is None:
+        J = core.s2dw_core_comp_Jmax(B, alpha)
+    K, P, bs = core.s2dw_core_init_kernels(J, B, alpha)
+    S = core.s2dw_core_init_directionality(B, N)
+    return {"B": B, "N": N, "alpha": alpha, "J": J, "K_gamma": K, "Phi2": P, "bl_scoeff": bs, "Slm": S}
