@@ -1,0 +1,399 @@
+"""Headline benchmark: S2DW analysis+synthesis pairs/s at B=1024, N=4, alpha=2,
+J=Jmax on one B200 (one map per pair, FP64 plain form).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one analysis (flm -> wav) followed by one synthesis (wav -> flm) of
+a seeded synthetic map, all inputs resident in HBM.  Prints one JSON line.
+Under torchrun each rank runs an independent replica (the transform has no
+cross-GPU exchange): scaling is weak, value = pairs of all ranks / max time.
+
+`e2e` times the same pair through the C-ABI host-buffer entry points
+(s2dwc_analysis_flm2wav_dynamic + s2dwc_synthesis_wav2flm_dynamic) with pinned
+host buffers, so every step includes the host<->device copies.
+
+`--impl reference` times the CPU restatement of the reference's algorithm
+(oracle/, the reference's Fortran cannot be compiled here) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "B=1024 N=4 analysis+synthesis pairs/s at recon err<=1e-10"
+UNIT = "pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--B", type=int, default=1024)
+    ap.add_argument("--N", type=int, default=4)
+    ap.add_argument("--alpha", type=float, default=2.0)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def contraction_flops_per_scale(B, N, alpha, J):
+    """Algorithmic FLOPs of the l-contractions per scale (analysis, synthesis):
+    4 flops per complex-by-real MAC, (l+1)^2 (m, m') pairs per l, times the
+    number of n with N+n odd (|n| <= min(N-1,l) for analysis, 0 <= n for
+    synthesis)."""
+    from s2dw_b200.core import band_limits
+
+    ana, syn = [], []
+    for j in range(J + 1):
+        hi, lo = band_limits(j, B, alpha)
+        fa = fs = 0.0
+        for l in range(lo + 1, hi):
+            k = min(N - 1, l)
+            na = sum(1 for n in range(-k, k + 1) if (N + n) % 2)
+            ns = sum(1 for n in range(0, k + 1) if (N + n) % 2)
+            fa += 4.0 * (l + 1) ** 2 * na
+            fs += 4.0 * (l + 1) ** 2 * ns
+        ana.append(fa)
+        syn.append(fs)
+    return ana, syn
+
+
+def measured_fp64_peak():
+    """FP64 reference rate on this GPU: best of 10 torch.matmul float64 4096^3
+    (cuBLAS DGEMM), TFLOP/s."""
+    import torch
+
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(B, N, alpha, budget_s=30.0):
+    """CPU restatement of the reference timed on the host cores on a bounded
+    sample: each O(bl^3) loop runs every s-th iteration; two strides s and
+    2s give t(s) = c + h/s, so the full pair costs c + h."""
+    from oracle import oracle as O
+
+    from s2dw_b200.workload import gaussian_flm, transform_setup
+
+    threads = min(os.cpu_count() or 1, 64)
+    O.set_num_threads(threads)
+    t = transform_setup(B, N, alpha)
+    flm = gaussian_flm(B, seed=0)
+    a = (t["K_gamma"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
+    s_ = (t["K_gamma"], t["Phi2"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
+
+    def run(stride):
+        O.set_sample_stride(stride)
+        t0 = time.perf_counter()
+        w, sc = O.analysis_dynamic(flm, *a)
+        O.synthesis_dynamic(w, sc, *s_)
+        return time.perf_counter() - t0
+
+    s1 = 32 if B >= 1024 else 8
+    t1 = run(s1)
+    t2 = run(s1 // 2)
+    O.set_sample_stride(1)
+    h = max((t2 - t1) / (1.0 / (s1 // 2) - 1.0 / s1), 0.0)
+    c = max(t1 - h / s1, 0.0)
+    full = c + h
+    return {"value": 1.0 / full, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"CPU restatement (C/OpenMP) of the reference loops at B={B} N={N}: every {s1}-th and "
+                       f"{s1 // 2}-th iteration of each O(bl^3) loop, fitted t(s)=c+h/s -> {full:.1f} s/pair "
+                       f"(sampled runs {t1:.1f}s, {t2:.1f}s)")}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    B, N, alpha = args.B, args.N, args.alpha
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(B, N, alpha)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian C_l=1/(l(l+1)) flm)",
+            "impl": "reference",
+            "config": {"workload": f"B={B} N={N} alpha={alpha:g} J=Jmax analysis+synthesis of one map",
+                       "B": B, "N": N, "alpha": alpha},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    del world
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    from s2dw_b200 import core
+    from s2dw_b200.device import Plan
+    from s2dw_b200.workload import gaussian_flm, transform_setup
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    B, N, alpha = args.B, args.N, args.alpha
+    t = transform_setup(B, N, alpha)
+    J = t["J"]
+    plan = Plan(B, N, alpha, J, device=local)
+    plan.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    bs = t["bl_scoeff"]
+    # a ring of inputs so consecutive steps never reuse the same flm
+    nring = 4
+    flms = [gaussian_flm(B, seed=rank * 1000 + i) for i in range(nring)]
+    d_flm = [torch.from_numpy(np.ascontiguousarray(f.T)).cuda() for f in flms]
+    d_wav = torch.empty(plan.wav_size, dtype=torch.float64, device="cuda")
+    d_sc = torch.empty(max(1, bs * bs), dtype=torch.complex128, device="cuda")
+    d_out = torch.empty_like(d_flm[0])
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        plan.analysis(d_flm[i % nring], d_wav, d_sc, stream)
+        plan.synthesis(d_wav, d_sc, d_out, stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    # reconstruction check of the last warm-up pair
+    recon = float(np.abs(d_out.cpu().numpy().T - flms[(args.warmup - 1) % nring]).max())
+
+    clocks = ClockSampler(local)
+    plan.set_timing(True)
+    plan.timing(reset=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    plan.set_timing(False)
+    elapsed = e0.elapsed_time(e1) / 1e3
+    elapsed = max_over_ranks(elapsed, world)
+    kt = plan.timing(reset=True)
+    pairs = args.steps * world
+    value = pairs / elapsed
+    la, ls = plan.launch_counts()
+
+    # ---- roofline of the dominant kernel (largest device-time share)
+    fp64_peak = measured_fp64_peak()
+    ana_f, syn_f = contraction_flops_per_scale(B, N, alpha, J)
+    dom = max(kt.items(), key=lambda kv: kv[1][1])
+    roofline = None
+    if dom[0] in ("lwalk", "mwalk"):
+        flops_per_pair = sum(ana_f) if dom[0] == "lwalk" else sum(syn_f)
+        n_launch, ms = dom[1]
+        per_launch_ms = ms / n_launch
+        launches_per_pair = n_launch / args.steps
+        achieved = flops_per_pair / launches_per_pair / (per_launch_ms / 1e3) / 1e12
+        roofline = {"kernel": dom[0], "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                    "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (fp64 has no entry in MEASURED_PEAKS.json)"}
+    else:
+        n_launch, ms = dom[1]
+        roofline = {"kernel": dom[0], "bound": "fp64", "achieved": None, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": None, "traffic": None,
+                    "note": "dominant kernel is a transform stage"}
+    kernel_ms = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps}
+                 for k, v in kt.items()}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        a_ = (t["K_gamma"], t["Slm"], J, B, N, bs, alpha)
+        wav_h = [torch.empty(core.wav_scale_shape(j, B, N, alpha)[::-1], dtype=torch.float64,
+                             pin_memory=True).numpy().T for j in range(J + 1)]
+        flm_h = [torch.empty((B, B), dtype=torch.complex128, pin_memory=True).numpy().T for _ in range(nring)]
+        for i in range(nring):
+            flm_h[i][...] = flms[i]
+        out_h = torch.empty((B, B), dtype=torch.complex128, pin_memory=True).numpy().T
+        sc_h = np.zeros((bs, bs), dtype=np.complex128, order="F")
+        import ctypes
+
+        from s2dw_b200._lib import check, lib
+
+        dp = ctypes.POINTER(ctypes.c_double)
+        L = lib()
+        wptr = (dp * (J + 1))(*[w.ctypes.data_as(dp) for w in wav_h])
+        K = np.asfortranarray(t["K_gamma"])
+        P = np.ascontiguousarray(t["Phi2"])
+        S = np.asfortranarray(t["Slm"])
+
+        def e2e_step(i):
+            check(L.s2dwc_analysis_flm2wav_dynamic(wptr, sc_h.ctypes.data_as(dp), flm_h[i % nring].ctypes.data_as(dp),
+                                                   K.ctypes.data_as(dp), S.ctypes.data_as(dp), J, B, N, bs, alpha))
+            check(L.s2dwc_synthesis_wav2flm_dynamic(out_h.ctypes.data_as(dp), wptr, sc_h.ctypes.data_as(dp),
+                                                    K.ctypes.data_as(dp), P.ctypes.data_as(dp), S.ctypes.data_as(dp),
+                                                    J, B, N, bs, alpha))
+
+        for i in range(2):
+            e2e_step(i)
+        barrier(world)
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            e2e_step(i)
+        te = time.perf_counter() - t0
+        te = max_over_ranks(te, world)
+        e2e_recon = float(np.abs(out_h - flm_h[(args.e2e_steps - 1) % nring]).max())
+        wav_bytes = 8 * plan.wav_size
+        e2e = {"value": args.e2e_steps * world / te, "unit": UNIT,
+               "h2d_bytes_per_step": 16 * B * B + wav_bytes + 16 * bs * bs,
+               "d2h_bytes_per_step": wav_bytes + 16 * bs * bs + 16 * B * B,
+               "recon_err": e2e_recon,
+               "api": "s2dwc_analysis_flm2wav_dynamic + s2dwc_synthesis_wav2flm_dynamic, pinned host buffers"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(B, N, alpha)
+        except Exception as ex:  # keep the GPU line even if the oracle is absent
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian C_l=1/(l(l+1)) flm, no dataset)",
+            "config": {"workload": f"B={B} N={N} alpha={alpha:g} J=Jmax={J} analysis+synthesis of one map per step",
+                       "B": B, "N": N, "alpha": alpha, "J": J, "form": "fp64 plain",
+                       "parallelism": f"replicas x{world} (no collective)",
+                       "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
+                       "recon_err": recon},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

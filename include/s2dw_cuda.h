@@ -175,6 +175,22 @@ int s2dwc_plan_synthesis(s2dwc_plan *plan, double *d_flm, const double *d_wav,
 /* Number of CUDA kernels one analysis / one synthesis launches. */
 int s2dwc_plan_launch_count(const s2dwc_plan *plan, int *analysis, int *synthesis);
 
+/* Per-kernel timing.  When enabled, every launch of the plan is bracketed by
+ * CUDA events on its stream; s2dwc_plan_timing() resolves the events
+ * (synchronising on them) and returns, for one kernel kind, the launches
+ * and total device milliseconds accumulated since the last reset. */
+#define S2DWC_KIND_LWALK 0     /* analysis contraction + gamma DFT */
+#define S2DWC_KIND_MWALK 1     /* synthesis contraction + harmonic sum */
+#define S2DWC_KIND_ANA_BETA 2  /* analysis beta transform */
+#define S2DWC_KIND_ANA_ALPHA 3 /* analysis alpha c2r transform */
+#define S2DWC_KIND_SYN_ALPHA 4 /* synthesis alpha r2c transform */
+#define S2DWC_KIND_SYN_BETA 5  /* synthesis gamma + beta transform and fold */
+#define S2DWC_KIND_OTHER 6     /* scaling coefficients, zeroing */
+#define S2DWC_KIND_COUNT 7
+int s2dwc_plan_set_timing(s2dwc_plan *plan, int enable);
+int s2dwc_plan_timing(s2dwc_plan *plan, int kind, long long *launches, double *total_ms);
+int s2dwc_plan_timing_reset(s2dwc_plan *plan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,7 +41,12 @@ SIGNATURES = {
     "s2dwc_plan_analysis": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_synthesis": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_launch_count": (_i, [_vp, _ip, _ip]),
+    "s2dwc_plan_set_timing": (_i, [_vp, _i]),
+    "s2dwc_plan_timing": (_i, [_vp, _i, _llp, _dp]),
+    "s2dwc_plan_timing_reset": (_i, [_vp]),
 }
+
+KERNEL_KINDS = ["lwalk", "mwalk", "ana_beta", "ana_alpha", "syn_alpha", "syn_beta", "other"]
 
 _lib = None
 

@@ -47,6 +47,11 @@ struct s2dwc_plan {
     double2 *hbFlm = nullptr, *hbSc = nullptr;
     int hbSc_n = 0;
     long long ws_bytes = 0;
+    // optional per-kernel CUDA-event timing: (kind, start, stop) per launch
+    bool timing = false;
+    std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> tev;
+    double t_ms[S2DWC_KIND_COUNT] = {0};
+    long long t_n[S2DWC_KIND_COUNT] = {0};
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
 
@@ -55,6 +60,10 @@ struct s2dwc_plan {
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
+        for (auto &t : tev) {
+            cudaEventDestroy(std::get<1>(t));
+            cudaEventDestroy(std::get<2>(t));
+        }
         for (void *p : allocs) cudaFree(p);
         cudaSetDevice(cur);
     }
@@ -217,6 +226,26 @@ struct DeviceGuard {
     }
 };
 
+// Brackets one launch with CUDA events on its stream when timing is on.
+struct KernelTimer {
+    s2dwc_plan *p;
+    int kind;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelTimer(s2dwc_plan *p_, int k, cudaStream_t s_) : p(p_), kind(k), s(s_)
+    {
+        if (p->timing && cudaEventCreate(&a) == cudaSuccess && cudaEventCreate(&b) == cudaSuccess)
+            cudaEventRecord(a, s);
+    }
+    ~KernelTimer()
+    {
+        if (a && b) {
+            cudaEventRecord(b, s);
+            p->tev.emplace_back(kind, a, b);
+        }
+    }
+};
+
 // Runs the analysis of every scale on `s`.
 int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s)
 {
@@ -238,7 +267,10 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         la.kappa = p->kappaA + (size_t)j * p->B * p->NP;
         la.flm = d_flm;
         la.Tg = p->wsC;
-        if ((st = launch_lwalk(la, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_LWALK, s);
+            if ((st = launch_lwalk(la, s))) return st;
+        }
 
         CztArgs ca{};
         ca.mode = CZT_ANA_BETA;
@@ -251,7 +283,10 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         ca.tw = p->tw[ca.czt.M];
         ca.in_c = p->wsC;
         ca.out_c = p->wsA;
-        if ((st = launch_czt(ca, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_ANA_BETA, s);
+            if ((st = launch_czt(ca, s))) return st;
+        }
 
         ca.mode = CZT_ANA_ALPHA;
         ca.rows = p->N * bl;  // (g, b pair)
@@ -260,8 +295,12 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         ca.in_c = p->wsA;
         ca.out_c = nullptr;
         ca.out_r = d_wav + p->wav_off[j];
-        if ((st = launch_czt(ca, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, s);
+            if ((st = launch_czt(ca, s))) return st;
+        }
     }
+    KernelTimer kt(p, S2DWC_KIND_OTHER, s);
     return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
 }
 
@@ -269,7 +308,10 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
                   cudaStream_t s)
 {
     int st;
-    if ((st = launch_zero(reinterpret_cast<double *>(d_flm), 2LL * p->B * p->B, s))) return st;
+    {
+        KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+        if ((st = launch_zero(reinterpret_cast<double *>(d_flm), 2LL * p->B * p->B, s))) return st;
+    }
     for (int j = 0; j <= p->J; j++) {
         const int bl = p->bl[j];
         CztArgs ca{};
@@ -284,7 +326,10 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ca.in_r = d_wav + p->wav_off[j];
         ca.out_c = p->wsA;
         ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
-        if ((st = launch_czt(ca, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, s);
+            if ((st = launch_czt(ca, s))) return st;
+        }
 
         ca.mode = CZT_SYN_BETA;
         ca.rows = p->NP * bl;
@@ -294,7 +339,10 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ca.in_r = nullptr;
         ca.out_c = p->wsC;
         ca.wq = p->wq[j];
-        if ((st = launch_czt(ca, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_SYN_BETA, s);
+            if ((st = launch_czt(ca, s))) return st;
+        }
 
         MwalkArgs ma{};
         ma.B = p->B;
@@ -311,8 +359,12 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ma.kappa = p->kappaS + (size_t)j * p->B * p->NP;
         ma.V2f = p->wsC;
         ma.flm = d_flm;
-        if ((st = launch_mwalk(ma, s))) return st;
+        {
+            KernelTimer kt(p, S2DWC_KIND_MWALK, s);
+            if ((st = launch_mwalk(ma, s))) return st;
+        }
     }
+    KernelTimer kt(p, S2DWC_KIND_OTHER, s);
     return launch_scaling_add(d_flm, d_scoeff, p->Phi2, p->B, p->bl_scoeff, s);
 }
 
@@ -461,6 +513,46 @@ int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
     for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? 1 : 0);
     if (synthesis) *synthesis = ns;
     return S2DWC_OK;
+}
+
+int s2dwc_plan_set_timing(s2dwc_plan *p, int enable)
+{
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "set_timing: null plan");
+    p->timing = enable != 0;
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_timing(s2dwc_plan *p, int kind, long long *launches, double *total_ms)
+{
+    if (!p || kind < 0 || kind >= S2DWC_KIND_COUNT)
+        return set_error(S2DWC_ERROR_ARG_INVALID, "timing: bad plan or kind %d", kind);
+    DeviceGuard dg(p->device);
+    for (auto &t : p->tev) {
+        float ms = 0.f;
+        S2DW_CUDA_TRY(cudaEventSynchronize(std::get<2>(t)));
+        S2DW_CUDA_TRY(cudaEventElapsedTime(&ms, std::get<1>(t), std::get<2>(t)));
+        p->t_ms[std::get<0>(t)] += ms;
+        p->t_n[std::get<0>(t)] += 1;
+        cudaEventDestroy(std::get<1>(t));
+        cudaEventDestroy(std::get<2>(t));
+    }
+    p->tev.clear();
+    if (launches) *launches = p->t_n[kind];
+    if (total_ms) *total_ms = p->t_ms[kind];
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_timing_reset(s2dwc_plan *p)
+{
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "timing_reset: null plan");
+    long long n;
+    double ms;
+    int st = s2dwc_plan_timing(p, 0, &n, &ms);
+    for (int k = 0; k < S2DWC_KIND_COUNT; k++) {
+        p->t_ms[k] = 0.0;
+        p->t_n[k] = 0;
+    }
+    return st;
 }
 
 int s2dwc_plan_analysis(s2dwc_plan *p, double *d_wav, double *d_scoeff, const double *d_flm, void *stream)

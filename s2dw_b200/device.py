@@ -53,6 +53,22 @@ class Plan:
         check(lib().s2dwc_plan_launch_count(self._h, ctypes.byref(a), ctypes.byref(s)))
         return a.value, s.value
 
+    def set_timing(self, enable=True):
+        check(lib().s2dwc_plan_set_timing(self._h, int(bool(enable))))
+
+    def timing(self, reset=False):
+        """{kind: (launches, total_ms)} accumulated since the last reset."""
+        from ._lib import KERNEL_KINDS
+
+        out = {}
+        for k, name in enumerate(KERNEL_KINDS):
+            n, ms = ctypes.c_longlong(0), ctypes.c_double(0.0)
+            check(lib().s2dwc_plan_timing(self._h, k, ctypes.byref(n), ctypes.byref(ms)))
+            out[name] = (n.value, ms.value)
+        if reset:
+            check(lib().s2dwc_plan_timing_reset(self._h))
+        return out
+
     def set_tables(self, K_gamma, Phi2, Slm, bl_scoeff):
         dp = ctypes.POINTER(ctypes.c_double)
         K = np.asfortranarray(K_gamma, dtype=np.float64)
