@@ -89,28 +89,42 @@ struct TwDev {
     double2 *hi = nullptr, *lo = nullptr;
 };
 
+// Tables of the plan use a padded row stride Bp = roundup(B, 32) so that
+// 32-wide tiles never read past a row.
 struct LwalkArgs {
-    int B, N, NP, bl, blo;
+    int B, Bp, N, NP, bl, blo;
     int nq[4];
-    const double *Om, *Acoef, *Stm;
+    const double *Acoef;  // [l*Bp + x]
+    const double *Stm;    // [l0*B + k]
     const int32_t *Ste;
-    const double *H;
-    const double *kappa;  // [l*NP + q] for this scale
-    const double2 *flm;   // (B,B) column-major
+    const double *G;      // [((l-blo-1)*NP + q)*Gs + m'] = Om(l,m') d^l_{m'n_q} K_j(l) s(l,n_q)
+    int Gs;               // roundup(bl, 32)
+    const double2 *F;     // [l*Bp + m] = Om(l,m) flm(l,m)
     double2 *Tg;          // [g][m][m'] N x bl x bl
 };
 
 struct MwalkArgs {
-    int B, N, NP, bl, blo;
+    int B, Bp, N, NP, bl, blo;
     int nq[4];
-    const double *Gam, *Bcoef, *Em;
+    const double *Bcoef;  // [l*Bp + m']
+    const double *Em;     // [l*B + m]
     const int32_t *Ee;
-    const double *H;
-    const double *kappa;  // [l*NP + q] for this scale
-    const double2 *V2f;   // [q][m][m'] NP x bl x bl
+    const double *G;      // [((l-blo-1)*NP + q)*Gs + m'] = Gam(l,m') d^l_{m'n_q} c_j(l,n_q)
+    int Gs;               // roundup(bl, 8)
+    const double2 *V2f;   // [(q*bl + m)*Vs + m']
+    int Vs;               // roundup(bl, 8)
     double2 *flm;         // (B,B) column-major, accumulated
 };
 
+// Per-scale factor tables G (see LwalkArgs / MwalkArgs), built at
+// set_tables time: out[((l-blo-1)*NP+q)*stride + x] = T[l*Bp+x] *
+// H[(l*8+nq)*B+x] * kappa[l*NP+q] for x <= l, x < bl; zero elsewhere.
+struct GprepArgs {
+    int B, Bp, NP, bl, blo, stride;
+    int nq[4];
+    const double *T, *H, *kappa;
+    double *out;
+};
 struct CztArgs {
     int mode, bl, N, NP, rows;
     int nq[4];
@@ -119,21 +133,21 @@ struct CztArgs {
     const double2 *in_c;   // complex input (Tg, Tb, V)
     const double *in_r;    // real input (wavelet coefficients)
     double2 *out_c;        // complex output (Tb, V, V2f)
+    int out_stride;        // row stride of V2f (CZT_SYN_BETA)
     double *out_r;         // real output (wavelet coefficients)
     const double *wq;      // quadrature weights (2bl) for CZT_SYN_BETA
     double scale;          // (4 pi^2/N)/(2bl-1) for CZT_SYN_ALPHA
 };
 
 int launch_lwalk(const LwalkArgs &a, cudaStream_t s);
+int launch_gprep(const GprepArgs &a, cudaStream_t s);
+// F[l*Bp + m] = Om[l*Bp + m] * flm[l + B*m] for m <= l < B, zero for m > l.
+int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp, cudaStream_t s);
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
 int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
 int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,
                        cudaStream_t s);
-int launch_static_scatter(double *wav_static, const double *wav_packed, int J, int B, int N,
-                          int jj, int bl, long long off, cudaStream_t s);
-int launch_static_gather(double *wav_packed, const double *wav_static, int J, int B, int N, int jj,
-                         int bl, long long off, cudaStream_t s);
 
 }  // namespace s2dw

@@ -63,35 +63,65 @@ __device__ __forceinline__ int warp_max_i(int v)
 #define S2DW_RENORM_EXP 400
 
 // ===========================================================================
+// Asynchronous global -> shared copies (16 bytes, L2 only)
+// ===========================================================================
+__device__ __forceinline__ void cp16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// ===========================================================================
 // Analysis: l-walk contraction fused with the gamma DFT
+//
+// CTA tile: 32 consecutive m' (lanes) x LW_W*S consecutive m (S per warp).
+// Each thread walks l for its S pairs (m', m); per step it needs a(l,m'),
+// G(l,m',q) (lane-distinct) and a(l,m), F(l,m) (warp-uniform broadcast),
+// staged LW_CH values of l at a time in a double-buffered cp.async pipeline.
 // ===========================================================================
 constexpr int LW_W = 4;    // warps per CTA
-constexpr int LW_CH = 16;  // l values staged per chunk (even)
+constexpr int LW_CH = 16;  // l values per staged chunk (even)
+
+template <int NP, int S>
+struct LwalkSmem {
+    static constexpr int WS = LW_W * S;
+    // per buffer, in doubles: F (complex, first for 16-byte alignment), Ap, G, Am
+    static constexpr int F_OFF = 0;
+    static constexpr int AP_OFF = F_OFF + 2 * LW_CH * WS;
+    static constexpr int G_OFF = AP_OFF + LW_CH * 32;
+    static constexpr int AM_OFF = G_OFF + LW_CH * NP * 32;
+    static constexpr int BUF = AM_OFF + LW_CH * WS;
+    static constexpr size_t BYTES = 2 * BUF * sizeof(double) + 8 * 16 * sizeof(double2);
+};
 
 template <int NP, int S>
 __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles_p)
 {
-    constexpr int WS = LW_W * S;
-    __shared__ double sAp[LW_CH][32];
-    __shared__ double sG[LW_CH][NP][32];
-    __shared__ double sAm[LW_CH][WS];
-    __shared__ double2 sF[LW_CH][WS];
-    __shared__ double2 sPh[8][16];  // exp(i pi n g / N) at [g][n+N-1]
+    using L = LwalkSmem<NP, S>;
+    constexpr int WS = L::WS;
+    extern __shared__ __align__(16) double lsm[];
+    double2 *sPh = reinterpret_cast<double2 *>(lsm + 2 * L::BUF);  // [g*16 + n+N-1]
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int pt = blockIdx.x % tiles_p, mt = blockIdx.x / tiles_p;
     const int p0 = pt * 32, m0 = mt * WS;
-    const int B = a.B, bl = a.bl, blo = a.blo, N = a.N;
+    const int B = a.B, Bp = a.Bp, bl = a.bl, blo = a.blo, N = a.N, Gs = a.Gs;
     const int mp = p0 + lane;
 
     for (int i = tid; i < N * (2 * N - 1); i += blockDim.x) {
-        int g = i / (2 * N - 1), n = i % (2 * N - 1) - (N - 1);
-        double s, c;
-        sincospi((double)(n * g) / (double)N, &s, &c);
-        sPh[g][n + N - 1] = make_double2(c, s);
+        const int g = i / (2 * N - 1), n = i % (2 * N - 1) - (N - 1);
+        double sn, cs;
+        sincospi((double)(n * g) / (double)N, &sn, &cs);
+        sPh[g * 16 + n + N - 1] = make_double2(cs, sn);
     }
 
-    // ---- per-pair start values (pair = (m', m) with m' = mp, m = m0+w*S+s)
+    // ---- per-pair start values; pair = (m' = mp, m = m0 + w*S + s)
     int l0[S];
     double st[S];
     int maxe = INT_MIN;
@@ -99,9 +129,8 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
     for (int s = 0; s < S; s++) {
         const int m = m0 + w * S + s;
         const bool valid = (mp < bl) && (m < bl);
-        const int L0 = max(mp, m), k = min(mp, m);
-        l0[s] = valid ? L0 : INT_MAX;
-        if (valid) maxe = max(maxe, (int)a.Ste[(size_t)L0 * B + k]);
+        l0[s] = valid ? max(mp, m) : INT_MAX;
+        if (valid) maxe = max(maxe, (int)a.Ste[(size_t)max(mp, m) * B + min(mp, m)]);
     }
     maxe = warp_max_i(maxe);
     int Kw = (maxe != INT_MIN && maxe < S2DW_SCALE_EXP) ? -maxe : 0;
@@ -110,8 +139,8 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
         const int m = m0 + w * S + s;
         st[s] = 0.0;
         if (l0[s] != INT_MAX) {
-            const int L0 = l0[s], k = min(mp, m);
-            double v = ldexp(a.Stm[(size_t)L0 * B + k], (int)a.Ste[(size_t)L0 * B + k] + Kw);
+            const size_t o = (size_t)l0[s] * B + min(mp, m);
+            double v = ldexp(a.Stm[o], (int)a.Ste[o] + Kw);
             if (mp >= m && ((mp - m) & 1)) v = -v;
             st[s] = v;
         }
@@ -129,20 +158,50 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
 
     const int lstart = max(p0, m0) & ~1;
     const int rampEnd = min(max(p0 + 31, m0 + WS - 1), bl - 1);
+    const int nchunks = (bl - lstart + LW_CH - 1) / LW_CH;
+
+    auto stage = [&](int c, int buf) {
+        const int lc = lstart + c * LW_CH;
+        double *b = lsm + buf * L::BUF;
+        // a(l, m') and a(l, m): 32 and WS doubles per row
+        for (int i = tid; i < LW_CH * (16 + WS / 2); i += blockDim.x) {
+            const int li = i / (16 + WS / 2), r = i % (16 + WS / 2), l = lc + li;
+            if (l >= bl) continue;
+            if (r < 16) cp16(b + L::AP_OFF + li * 32 + 2 * r, a.Acoef + (size_t)l * Bp + p0 + 2 * r);
+            else cp16(b + L::AM_OFF + li * WS + 2 * (r - 16), a.Acoef + (size_t)l * Bp + m0 + 2 * (r - 16));
+        }
+        if (lc + LW_CH - 1 > blo) {
+            for (int i = tid; i < LW_CH * (NP * 16 + WS); i += blockDim.x) {
+                const int li = i / (NP * 16 + WS), r = i % (NP * 16 + WS), l = lc + li;
+                if (l >= bl || l <= blo) continue;
+                if (r < NP * 16) {
+                    const int q = r >> 4, c2 = r & 15;
+                    cp16(b + L::G_OFF + (li * NP + q) * 32 + 2 * c2,
+                         a.G + ((size_t)(l - blo - 1) * NP + q) * Gs + p0 + 2 * c2);
+                } else {
+                    const int c1 = r - NP * 16;
+                    cp16(b + L::F_OFF + 2 * (li * WS + c1), a.F + (size_t)l * Bp + m0 + c1);
+                }
+            }
+        }
+    };
 
     // One recurrence step at chunk row li (l parity PAR).
-    auto step = [&](const int li, const int l, auto par_tag, const bool inj, const bool accum) {
+    auto step = [&](const double *b, const int li, const int l, auto par_tag, const bool inj, const bool accum) {
         constexpr int PAR = decltype(par_tag)::value;
-        const double ap = sAp[li][lane];
+        const double ap = b[L::AP_OFF + li * 32 + lane];
         double g[NP];
+        if (accum) {
 #pragma unroll
-        for (int q = 0; q < NP; q++) g[q] = sG[li][q][lane];
+            for (int q = 0; q < NP; q++) g[q] = b[L::G_OFF + (li * NP + q) * 32 + lane];
+        }
+        const double2 *Fr = reinterpret_cast<const double2 *>(b + L::F_OFF) + li * WS + w * S;
+        const double *Amr = b + L::AM_OFF + li * WS + w * S;
 #pragma unroll
         for (int s = 0; s < S; s++) {
             if (inj && l == l0[s]) e[s] = st[s];
-            const double am = sAm[li][w * S + s];
             if (accum) {
-                const double2 F = sF[li][w * S + s];
+                const double2 F = Fr[s];
                 const double xr = e[s] * F.x, xi = e[s] * F.y;
 #pragma unroll
                 for (int q = 0; q < NP; q++) {
@@ -150,7 +209,7 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
                     acc[PAR][s][q].y = fma(xi, g[q], acc[PAR][s][q].y);
                 }
             }
-            const double p = am * ap;
+            const double p = Amr[s] * ap;
             const double en = fma(-p, e[s], -ep[s]);
             ep[s] = e[s];
             e[s] = en;
@@ -159,43 +218,28 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
     using P0 = std::integral_constant<int, 0>;
     using P1 = std::integral_constant<int, 1>;
 
-    for (int lc = lstart; lc < bl; lc += LW_CH) {
+    if (nchunks > 0) stage(0, 0);
+    cp_commit();
+    for (int c = 0; c < nchunks; c++) {
+        if (c + 1 < nchunks) stage(c + 1, (c + 1) & 1);
+        cp_commit();
+        cp_wait<1>();
         __syncthreads();
-        // ---- stage chunk [lc, lc+LW_CH)
-        for (int i = tid; i < LW_CH * 32; i += blockDim.x) {
-            const int li = i >> 5, t = i & 31, l = lc + li, x = p0 + t;
-            const bool ok = (l < bl) && (x < bl) && (x <= l);
-            const size_t o = (size_t)l * B + x;
-            const double om = ok ? a.Om[o] : 0.0;
-            sAp[li][t] = ok ? a.Acoef[o] : 0.0;
-#pragma unroll
-            for (int q = 0; q < NP; q++)
-                sG[li][q][t] = ok ? om * a.H[((size_t)l * 8 + a.nq[q]) * B + x] * a.kappa[(size_t)l * NP + q]
-                                  : 0.0;
-        }
-        for (int i = tid; i < LW_CH * WS; i += blockDim.x) {
-            const int t = i / LW_CH, li = i % LW_CH, l = lc + li, m = m0 + t;
-            const bool ok = (l < bl) && (m < bl) && (m <= l);
-            const size_t o = (size_t)l * B + m;
-            sAm[li][t] = ok ? a.Acoef[o] : 0.0;
-            double2 f = ok ? a.flm[(size_t)l + (size_t)B * m] : make_double2(0.0, 0.0);
-            const double om = ok ? a.Om[o] : 0.0;
-            sF[li][t] = make_double2(om * f.x, om * f.y);
-        }
-        __syncthreads();
+        const double *b = lsm + (c & 1) * L::BUF;
+        const int lc = lstart + c * LW_CH;
         const int nl = min(LW_CH, bl - lc);
         if (lc > rampEnd && lc > blo && nl == LW_CH) {
 #pragma unroll 1
             for (int li = 0; li < LW_CH; li += 2) {
-                step(li, lc + li, P0{}, false, true);
-                step(li + 1, lc + li + 1, P1{}, false, true);
+                step(b, li, lc + li, P0{}, false, true);
+                step(b, li + 1, lc + li + 1, P1{}, false, true);
             }
         } else {
 #pragma unroll 1
             for (int li = 0; li < nl; li += 2) {
                 const int l = lc + li;
-                step(li, l, P0{}, l <= rampEnd, l > blo);
-                if (li + 1 < nl) step(li + 1, l + 1, P1{}, l + 1 <= rampEnd, l + 1 > blo);
+                step(b, li, l, P0{}, l <= rampEnd, l > blo);
+                if (li + 1 < nl) step(b, li + 1, l + 1, P1{}, l + 1 <= rampEnd, l + 1 > blo);
             }
         }
         if (Kw > 0) {  // keep scaled values in range (warp-uniform)
@@ -219,8 +263,8 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
                 Kw -= R;
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     // ---- epilogue: T(m,m',+-n) from even/odd-l sums, then the gamma DFT
     // T(+n) = i^{n-m} conj(eta) (E+O), T(-n) = i^{-n-m} (-1)^{m'+n} eta (E-O),
@@ -252,35 +296,91 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
 #pragma unroll
             for (int q = 0; q < NP; q++) {
                 const int n = a.nq[q];
-                y = cadd(y, cmul(Tp[q], sPh[gg][n + N - 1]));
-                if (n != 0) y = cadd(y, cmul(Tm[q], sPh[gg][-n + N - 1]));
+                y = cadd(y, cmul(Tp[q], sPh[gg * 16 + n + N - 1]));
+                if (n != 0) y = cadd(y, cmul(Tm[q], sPh[gg * 16 - n + N - 1]));
             }
             a.Tg[((size_t)gg * bl + m) * bl + mp] = y;
         }
     }
 }
 
+// Per-scale factor tables for the contraction kernels (built once per set of
+// kernel tables).
+__global__ void gprep_kernel(GprepArgs a)
+{
+    const int nl = a.bl - a.blo - 1;
+    const long long total = (long long)nl * a.NP * a.stride;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % a.stride);
+        const long long r = i / a.stride;
+        const int q = (int)(r % a.NP), l = a.blo + 1 + (int)(r / a.NP);
+        double v = 0.0;
+        if (x <= l && x < a.bl)
+            v = a.T[(size_t)l * a.Bp + x] * a.H[((size_t)l * 8 + a.nq[q]) * a.B + x] * a.kappa[(size_t)l * a.NP + q];
+        a.out[i] = v;
+    }
+}
+
+// F[l*Bp + m] = Om[l*Bp+m] flm[l + B m]: transpose of the column-major flm
+// through a 32x32 shared tile.
+__global__ void fprep_kernel(double2 *F, const double2 *flm, const double *Om, int B, int Bp)
+{
+    __shared__ double2 tile[32][33];
+    const int l0 = blockIdx.x * 32, mb = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int k = ty; k < 32; k += 8) {
+        const int l = l0 + tx, m = mb + k;
+        tile[k][tx] = (l < B && m < B) ? flm[(size_t)l + (size_t)B * m] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int l = l0 + k, m = mb + tx;
+        if (l < B && m < Bp) {
+            double2 v = make_double2(0.0, 0.0);
+            if (m <= l && m < B) v = cscale(tile[tx][k], Om[(size_t)l * Bp + m]);
+            F[(size_t)l * Bp + m] = v;
+        }
+    }
+}
+
 // ===========================================================================
 // Synthesis: m'-walk contraction and harmonic accumulation
+//
+// CTA tile: 32 consecutive l (lanes) x MW_W*Q consecutive m (Q per warp).
+// Each thread walks m' down from min(l_tile_max, bl-1) to 0 for its Q pairs
+// (l, m).  Staged per chunk of MW_CH m' values (aligned to MW_CH): the
+// lane-distinct rows b(l, m') and G(l, m', q) (each thread copies its row to
+// registers) and the broadcast V2f(m, m', q).
 // ===========================================================================
 constexpr int MW_W = 4;
 constexpr int MW_CH = 8;
+constexpr int MW_RS = MW_CH + 2;  // padded row stride (conflict-free 16-byte row loads)
+
+template <int NP, int Q>
+struct MwalkSmem {
+    static constexpr int WQ = MW_W * Q;
+    static constexpr int V_OFF = 0;                          // double2 [NP][WQ][MW_CH]
+    static constexpr int B_OFF = V_OFF + 2 * NP * WQ * MW_CH;  // double [32][MW_RS]
+    static constexpr int G_OFF = B_OFF + 32 * MW_RS;           // double [NP][32][MW_RS]
+    static constexpr int BUF = G_OFF + NP * 32 * MW_RS;
+    static constexpr size_t BYTES = 2 * BUF * sizeof(double);
+};
 
 template <int NP, int Q>
 __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles_m)
 {
-    constexpr int WQ = MW_W * Q;
-    __shared__ double sB[MW_CH][32];
-    __shared__ double sGH[MW_CH][NP][32];
-    __shared__ double2 sV[MW_CH][NP][WQ];
+    using L = MwalkSmem<NP, Q>;
+    constexpr int WQ = L::WQ;
+    extern __shared__ __align__(16) double msm[];
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int mt = blockIdx.x % tiles_m, lt = blockIdx.x / tiles_m;
-    const int B = a.B, bl = a.bl, blo = a.blo;
+    const int B = a.B, Bp = a.Bp, bl = a.bl, blo = a.blo, Gs = a.Gs, Vs = a.Vs;
     const int lbase = blo + 1 + lt * 32, mbase = mt * WQ;
-    if (mbase > min(lbase + 31, bl - 1)) return;  // tile entirely above the diagonal m <= l
-    const int l = lbase + lane;
     const int MH = min(lbase + 31, bl - 1);
+    if (mbase > MH) return;  // tile entirely above the diagonal m <= l
+    const int l = lbase + lane;
 
     double st[Q], mq[Q];
     bool val[Q];
@@ -299,7 +399,7 @@ __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles
         const int m = mbase + w * Q + q;
         st[q] = 0.0;
         if (val[q]) {
-            double v = ldexp(a.Em[(size_t)l * B + m], (int)a.Ee[(size_t)l * B + m] + Kw);
+            const double v = ldexp(a.Em[(size_t)l * B + m], (int)a.Ee[(size_t)l * B + m] + Kw);
             st[q] = ((l - m) & 1) ? -v : v;
         }
     }
@@ -311,48 +411,78 @@ __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles
         acc[q] = make_double2(0.0, 0.0);
     }
 
-    for (int mc = MH; mc >= 0; mc -= MW_CH) {
-        __syncthreads();
-        for (int i = tid; i < MW_CH * 32; i += blockDim.x) {
-            const int t = i / MW_CH, ci = i % MW_CH, ll = lbase + t, mpv = mc - ci;
-            const bool ok = (mpv >= 0) && (ll < bl) && (mpv <= ll);
-            const size_t o = (size_t)ll * B + mpv;
-            sB[ci][t] = ok ? a.Bcoef[o] : 0.0;
-            const double gm = ok ? a.Gam[o] : 0.0;
-#pragma unroll
-            for (int q = 0; q < NP; q++)
-                sGH[ci][q][t] = ok ? gm * a.H[((size_t)ll * 8 + a.nq[q]) * B + mpv] * a.kappa[(size_t)ll * NP + q]
-                                   : 0.0;
+    const int ctop = MH / MW_CH;  // chunks ctop, ctop-1, ..., 0 cover m' = MH .. 0
+
+    auto stage = [&](int c, int buf) {
+        double *b = msm + buf * L::BUF;
+        const int c0 = c * MW_CH;
+        // rows of b(l, m') and G(l, m', q): MW_CH/2 copies per row
+        for (int i = tid; i < (1 + NP) * 32 * (MW_CH / 2); i += blockDim.x) {
+            const int k = i % (MW_CH / 2), row = i / (MW_CH / 2), t = row % 32, q = row / 32;
+            const int ll = lbase + t;
+            double *dst = (q == 0) ? b + L::B_OFF + t * MW_RS + 2 * k
+                                   : b + L::G_OFF + ((q - 1) * 32 + t) * MW_RS + 2 * k;
+            if (ll < bl) {
+                const double *src = (q == 0) ? a.Bcoef + (size_t)ll * Bp + c0 + 2 * k
+                                             : a.G + ((size_t)(ll - blo - 1) * NP + (q - 1)) * Gs + c0 + 2 * k;
+                cp16(dst, src);
+            } else {
+                dst[0] = 0.0;
+                dst[1] = 0.0;
+            }
         }
-        for (int i = tid; i < MW_CH * WQ * NP; i += blockDim.x) {
-            const int ci = i % MW_CH, r = i / MW_CH, u = r % WQ, q = r / WQ;
-            const int m = mbase + u, mpv = mc - ci;
-            const bool ok = (mpv >= 0) && (m < bl);
-            sV[ci][q][u] = ok ? a.V2f[((size_t)q * bl + m) * bl + mpv] : make_double2(0.0, 0.0);
+        // V2f(m, m', q) for the tile's m: MW_CH complex per (q, m)
+        for (int i = tid; i < NP * WQ * MW_CH; i += blockDim.x) {
+            const int k = i % MW_CH, r = i / MW_CH, u = r % WQ, q = r / WQ;
+            const int m = mbase + u;
+            double *dst = b + L::V_OFF + 2 * ((q * WQ + u) * MW_CH + k);
+            if (m < bl) cp16(dst, a.V2f + ((size_t)q * bl + m) * Vs + c0 + k);
+            else { dst[0] = 0.0; dst[1] = 0.0; }
         }
+    };
+
+    stage(ctop, 0);
+    cp_commit();
+    for (int c = ctop, it = 0; c >= 0; c--, it++) {
+        if (c > 0) stage(c - 1, (it + 1) & 1);
+        cp_commit();
+        cp_wait<1>();
         __syncthreads();
-        const int nc = min(MW_CH, mc + 1);
-        const bool ramp = (mc >= lbase);
-#pragma unroll 1
-        for (int ci = 0; ci < nc; ci++) {
-            const int mpv = mc - ci;
-            const double bb = sB[ci][lane];
-            double gh[NP];
+        const double *b = msm + (it & 1) * L::BUF;
+        const int c0 = c * MW_CH;
+        // this thread's rows into registers
+        double br[MW_CH], gr[NP][MW_CH];
 #pragma unroll
-            for (int q = 0; q < NP; q++) gh[q] = sGH[ci][q][lane];
+        for (int k = 0; k < MW_CH; k += 2) {
+            const double2 v = *reinterpret_cast<const double2 *>(b + L::B_OFF + lane * MW_RS + k);
+            br[k] = v.x;
+            br[k + 1] = v.y;
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                const double2 u = *reinterpret_cast<const double2 *>(b + L::G_OFF + (q * 32 + lane) * MW_RS + k);
+                gr[q][k] = u.x;
+                gr[q][k + 1] = u.y;
+            }
+        }
+        const double2 *Vb = reinterpret_cast<const double2 *>(b + L::V_OFF);
+        const bool ramp = (c0 + MW_CH - 1 >= lbase);
+#pragma unroll
+        for (int k = MW_CH - 1; k >= 0; k--) {
+            const int mpv = c0 + k;
+            if (mpv > MH) continue;  // above the top of this tile (warp-uniform)
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 if (ramp && mpv == l) e[q] = st[q];
                 double zr = 0.0, zi = 0.0;
 #pragma unroll
-                for (int k = 0; k < NP; k++) {
-                    const double2 v = sV[ci][k][w * Q + q];
-                    zr = fma(gh[k], v.x, zr);
-                    zi = fma(gh[k], v.y, zi);
+                for (int kq = 0; kq < NP; kq++) {
+                    const double2 v = Vb[(kq * WQ + w * Q + q) * MW_CH + k];
+                    zr = fma(gr[kq][k], v.x, zr);
+                    zi = fma(gr[kq][k], v.y, zi);
                 }
                 acc[q].x = fma(e[q], zr, acc[q].x);
                 acc[q].y = fma(e[q], zi, acc[q].y);
-                const double p = mq[q] * bb;
+                const double p = mq[q] * br[k];
                 const double en = fma(p, e[q], -ep[q]);
                 ep[q] = e[q];
                 e[q] = en;
@@ -375,8 +505,9 @@ __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles
                 Kw -= R;
             }
         }
+        __syncthreads();
     }
-    // flm(l,m) += i^m * acc (the eta and i^{-n} phases are folded into kappa)
+    // flm(l,m) += i^m * acc (the eta and i^{-n} phases are folded into G)
     const double sc = ldexp(1.0, -Kw);
 #pragma unroll
     for (int q = 0; q < Q; q++) {
@@ -623,7 +754,7 @@ __global__ void __launch_bounds__(512) czt_kernel(CztArgs a)
                 if ((m + a.nq[q]) & 1) z = make_double2(-z.x, -z.y);
                 y = cadd(y, z);
             }
-            a.out_c[((size_t)q * bl + m) * bl + mpv] = y;
+            a.out_c[((size_t)q * bl + m) * a.out_stride + mpv] = y;
         }
         break;
     }
@@ -659,12 +790,20 @@ __global__ void scaling_add_kernel(double2 *flm, const double2 *sc, const double
 // ===========================================================================
 // Launchers
 // ===========================================================================
-template <int NP>
+template <int NP, int S>
 static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 {
-    constexpr int S = (NP <= 2) ? 4 : 4;
-    const int tiles_p = (a.bl + 31) / 32, tiles_m = (a.bl + LW_W * S - 1) / (LW_W * S);
-    lwalk_kernel<NP, S><<<tiles_p * tiles_m, LW_W * 32, 0, s>>>(a, tiles_p);
+    using L = LwalkSmem<NP, S>;
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(lwalk_kernel<NP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::BYTES));
+        attr[dev] = true;
+    }
+    const int tiles_p = (a.bl + 31) / 32, tiles_m = (a.bl + L::WS - 1) / L::WS;
+    lwalk_kernel<NP, S><<<tiles_p * tiles_m, LW_W * 32, L::BYTES, s>>>(a, tiles_p);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
@@ -672,22 +811,30 @@ static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 int launch_lwalk(const LwalkArgs &a, cudaStream_t s)
 {
     switch (a.NP) {
-    case 1: return launch_lwalk_np<1>(a, s);
-    case 2: return launch_lwalk_np<2>(a, s);
-    case 3: return launch_lwalk_np<3>(a, s);
-    case 4: return launch_lwalk_np<4>(a, s);
+    case 1: return launch_lwalk_np<1, 4>(a, s);
+    case 2: return launch_lwalk_np<2, 4>(a, s);
+    case 3: return launch_lwalk_np<3, 4>(a, s);
+    case 4: return launch_lwalk_np<4, 4>(a, s);
     }
     return set_error(S2DWC_ERROR_SIZE_INVALID, "lwalk: unsupported N=%d (N<=8)", a.N);
 }
 
-template <int NP>
+template <int NP, int Q>
 static int launch_mwalk_np(const MwalkArgs &a, cudaStream_t s)
 {
-    constexpr int Q = 8;
+    using L = MwalkSmem<NP, Q>;
     const int nl = a.bl - a.blo - 1;
     if (nl <= 0) return S2DWC_OK;
-    const int tiles_l = (nl + 31) / 32, tiles_m = (a.bl + MW_W * Q - 1) / (MW_W * Q);
-    mwalk_kernel<NP, Q><<<tiles_l * tiles_m, MW_W * 32, 0, s>>>(a, tiles_m);
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(mwalk_kernel<NP, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::BYTES));
+        attr[dev] = true;
+    }
+    const int tiles_l = (nl + 31) / 32, tiles_m = (a.bl + L::WQ - 1) / L::WQ;
+    mwalk_kernel<NP, Q><<<tiles_l * tiles_m, MW_W * 32, L::BYTES, s>>>(a, tiles_m);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
@@ -695,12 +842,31 @@ static int launch_mwalk_np(const MwalkArgs &a, cudaStream_t s)
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
 {
     switch (a.NP) {
-    case 1: return launch_mwalk_np<1>(a, s);
-    case 2: return launch_mwalk_np<2>(a, s);
-    case 3: return launch_mwalk_np<3>(a, s);
-    case 4: return launch_mwalk_np<4>(a, s);
+    case 1: return launch_mwalk_np<1, 8>(a, s);
+    case 2: return launch_mwalk_np<2, 8>(a, s);
+    case 3: return launch_mwalk_np<3, 8>(a, s);
+    case 4: return launch_mwalk_np<4, 8>(a, s);
     }
     return set_error(S2DWC_ERROR_SIZE_INVALID, "mwalk: unsupported N=%d (N<=8)", a.N);
+}
+
+int launch_gprep(const GprepArgs &a, cudaStream_t s)
+{
+    const long long total = (long long)(a.bl - a.blo - 1) * a.NP * a.stride;
+    if (total <= 0) return S2DWC_OK;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    gprep_kernel<<<(int)blocks, 256, 0, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp, cudaStream_t s)
+{
+    dim3 grid((B + 31) / 32, (Bp + 31) / 32), block(32, 8);
+    fprep_kernel<<<grid, block, 0, s>>>(F, flm, Om, B, Bp);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
 }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)

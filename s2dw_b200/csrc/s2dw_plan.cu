@@ -23,7 +23,7 @@
 using namespace s2dw;
 
 struct s2dwc_plan {
-    int B = 0, N = 0, J = 0, device = 0, form = 0, NP = 0;
+    int B = 0, Bp = 0, N = 0, J = 0, device = 0, form = 0, NP = 0;
     double alpha = 0.0;
     int nq[4] = {0, 0, 0, 0};
     int bl_scoeff = 0;
@@ -38,8 +38,12 @@ struct s2dwc_plan {
     std::vector<std::array<CztDev, 4>> czt;
     std::map<int, TwDev> tw;
     std::vector<double *> wq;  // quadrature weights per scale
-    // caller tables
+    // caller tables folded into per-scale factor tables
     double *kappaA = nullptr, *kappaS = nullptr, *Phi2 = nullptr;
+    double *Ga = nullptr, *Gsyn = nullptr;       // all scales, see LwalkArgs/MwalkArgs
+    std::vector<long long> ga_off, gs_off;       // per-scale offsets (doubles)
+    std::vector<int> ga_stride, gs_stride;
+    double2 *Fw = nullptr;                       // per-call F table [l*Bp + m]
     // workspaces
     double2 *wsA = nullptr, *wsC = nullptr;
     // device buffers of the host-buffer entry points (allocated on first use)
@@ -108,10 +112,19 @@ int plan_build(s2dwc_plan *p)
     }
     RecTables t;
     build_rec_tables(B, t);
+    // row-padded copies (stride Bp) of the tables read by 32-wide tiles
+    const int Bp = (B + 31) / 32 * 32;
+    p->Bp = Bp;
+    auto pad = [&](const std::vector<double> &v) {
+        std::vector<double> o((size_t)B * Bp, 0.0);
+        for (int l = 0; l < B; l++)
+            std::copy(v.begin() + (size_t)l * B, v.begin() + (size_t)(l + 1) * B, o.begin() + (size_t)l * Bp);
+        return o;
+    };
     int st;
-    if ((st = dev_upload(p, &p->Om, t.Om)) || (st = dev_upload(p, &p->Acoef, t.Acoef)) ||
+    if ((st = dev_upload(p, &p->Om, pad(t.Om))) || (st = dev_upload(p, &p->Acoef, pad(t.Acoef))) ||
         (st = dev_upload(p, &p->Stm, t.Stm)) || (st = dev_upload(p, &p->Ste, t.Ste)) ||
-        (st = dev_upload(p, &p->Gam, t.Gam)) || (st = dev_upload(p, &p->Bcoef, t.Bcoef)) ||
+        (st = dev_upload(p, &p->Gam, pad(t.Gam))) || (st = dev_upload(p, &p->Bcoef, pad(t.Bcoef))) ||
         (st = dev_upload(p, &p->Em, t.Em)) || (st = dev_upload(p, &p->Ee, t.Ee)) ||
         (st = dev_upload(p, &p->H, t.H)))
         return st;
@@ -169,8 +182,25 @@ int plan_build(s2dwc_plan *p)
         (st = dev_alloc(p, &p->kappaS, (size_t)(J + 1) * B * p->NP)) ||
         (st = dev_alloc(p, &p->Phi2, (size_t)B)))
         return st;
-    // workspaces: wsA holds Tb / V (N x bl x 2bl), wsC holds Tg / V2f
-    const size_t nA = (size_t)N * B * 2 * B, nC = (size_t)std::max(N, p->NP) * B * B;
+    // per-scale factor tables: rows l in (blo, bl)
+    long long na = 0, ns = 0;
+    for (int j = 0; j <= J; j++) {
+        const int nl = std::max(0, p->bl[j] - p->blo[j] - 1);
+        p->ga_stride.push_back((p->bl[j] + 31) / 32 * 32);
+        p->gs_stride.push_back((p->bl[j] + 7) / 8 * 8);
+        p->ga_off.push_back(na);
+        p->gs_off.push_back(ns);
+        na += (long long)nl * p->NP * p->ga_stride[j];
+        ns += (long long)nl * p->NP * p->gs_stride[j];
+    }
+    if ((st = dev_alloc(p, &p->Ga, (size_t)std::max(1LL, na))) ||
+        (st = dev_alloc(p, &p->Gsyn, (size_t)std::max(1LL, ns))) ||
+        (st = dev_alloc(p, &p->Fw, (size_t)B * Bp)))
+        return st;
+    // workspaces: wsA holds Tb / V (N x bl x 2bl), wsC holds Tg (N x bl x bl)
+    // and V2f (NP x bl x roundup(bl,8))
+    const size_t nA = (size_t)N * B * 2 * B;
+    const size_t nC = std::max((size_t)N * B * B, (size_t)p->NP * B * ((B + 7) / 8 * 8));
     if ((st = dev_alloc(p, &p->wsA, nA)) || (st = dev_alloc(p, &p->wsC, nC))) return st;
     return S2DWC_OK;
 }
@@ -250,22 +280,26 @@ struct KernelTimer {
 int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s)
 {
     int st;
+    {
+        KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+        if ((st = launch_fprep(p->Fw, d_flm, p->Om, p->B, p->Bp, s))) return st;
+    }
     for (int j = 0; j <= p->J; j++) {
         const int bl = p->bl[j];
         LwalkArgs la{};
         la.B = p->B;
+        la.Bp = p->Bp;
         la.N = p->N;
         la.NP = p->NP;
         la.bl = bl;
         la.blo = p->blo[j];
         std::memcpy(la.nq, p->nq, sizeof(la.nq));
-        la.Om = p->Om;
         la.Acoef = p->Acoef;
         la.Stm = p->Stm;
         la.Ste = p->Ste;
-        la.H = p->H;
-        la.kappa = p->kappaA + (size_t)j * p->B * p->NP;
-        la.flm = d_flm;
+        la.G = p->Ga + p->ga_off[j];
+        la.Gs = p->ga_stride[j];
+        la.F = p->Fw;
         la.Tg = p->wsC;
         {
             KernelTimer kt(p, S2DWC_KIND_LWALK, s);
@@ -338,6 +372,7 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ca.in_c = p->wsA;
         ca.in_r = nullptr;
         ca.out_c = p->wsC;
+        ca.out_stride = p->gs_stride[j];
         ca.wq = p->wq[j];
         {
             KernelTimer kt(p, S2DWC_KIND_SYN_BETA, s);
@@ -346,18 +381,19 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
 
         MwalkArgs ma{};
         ma.B = p->B;
+        ma.Bp = p->Bp;
         ma.N = p->N;
         ma.NP = p->NP;
         ma.bl = bl;
         ma.blo = p->blo[j];
         std::memcpy(ma.nq, p->nq, sizeof(ma.nq));
-        ma.Gam = p->Gam;
         ma.Bcoef = p->Bcoef;
         ma.Em = p->Em;
         ma.Ee = p->Ee;
-        ma.H = p->H;
-        ma.kappa = p->kappaS + (size_t)j * p->B * p->NP;
+        ma.G = p->Gsyn + p->gs_off[j];
+        ma.Gs = p->gs_stride[j];
         ma.V2f = p->wsC;
+        ma.Vs = p->gs_stride[j];
         ma.flm = d_flm;
         {
             KernelTimer kt(p, S2DWC_KIND_MWALK, s);
@@ -491,6 +527,28 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
         S2DW_CUDA_TRY(cudaMemcpy(p->Phi2, Phi2, (size_t)B * sizeof(double), cudaMemcpyHostToDevice));
     else
         S2DW_CUDA_TRY(cudaMemset(p->Phi2, 0, (size_t)B * sizeof(double)));
+    for (int j = 0; j <= J; j++) {
+        GprepArgs g{};
+        g.B = B;
+        g.Bp = p->Bp;
+        g.NP = NP;
+        g.bl = p->bl[j];
+        g.blo = p->blo[j];
+        std::memcpy(g.nq, p->nq, sizeof(g.nq));
+        g.H = p->H;
+        g.T = p->Om;
+        g.kappa = p->kappaA + (size_t)j * B * NP;
+        g.stride = p->ga_stride[j];
+        g.out = p->Ga + p->ga_off[j];
+        int st = launch_gprep(g, 0);
+        if (st) return st;
+        g.T = p->Gam;
+        g.kappa = p->kappaS + (size_t)j * B * NP;
+        g.stride = p->gs_stride[j];
+        g.out = p->Gsyn + p->gs_off[j];
+        if ((st = launch_gprep(g, 0))) return st;
+    }
+    S2DW_CUDA_TRY(cudaDeviceSynchronize());
     p->bl_scoeff = bl_scoeff;
     p->tables_set = true;
     return S2DWC_OK;
@@ -508,7 +566,7 @@ long long s2dwc_plan_workspace_bytes(const s2dwc_plan *p) { return p ? p->ws_byt
 int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
 {
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "launch_count: null plan");
-    if (analysis) *analysis = 3 * (p->J + 1) + 1;
+    if (analysis) *analysis = 3 * (p->J + 1) + 2;
     int ns = 2;
     for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? 1 : 0);
     if (synthesis) *synthesis = ns;
