@@ -459,6 +459,16 @@ void build_czt_tables(const CztSpec &c, std::vector<double2> &pre, std::vector<d
         Hf[k] = make_double2((double)(h[k].real() / c.M), (double)(h[k].imag() / c.M));
 }
 
+void build_beta_twiddles(int bl, std::vector<double2> &tw)
+{
+    const ld pi = 3.141592653589793238462643383279502884L;
+    tw.resize(bl);
+    for (int k = 0; k < bl; k++) {
+        ld a = pi * (ld)k / (ld)(4LL * bl);
+        tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+}
+
 void build_twiddles(int M, std::vector<double2> &hi, std::vector<double2> &lo)
 {
     const ld pi = 3.141592653589793238462643383279502884L;

@@ -69,6 +69,8 @@ struct CztSpec {
 int czt_size(int K, int Bout);  // power of two M >= max(16, K+Bout-1)
 void build_czt_tables(const CztSpec &c, std::vector<double2> &pre, std::vector<double2> &post,
                       std::vector<double2> &Hf);
+// exp(i pi k / (4 bl)) for k < bl: the pre/post twiddle of the FFT beta modes.
+void build_beta_twiddles(int bl, std::vector<double2> &tw);
 // Two-level twiddle tables for a power-of-two FFT of size M:
 // W_M^x = hi[x >> 6] * lo[x & 63], W_M = exp(-2 pi i / M).
 void build_twiddles(int M, std::vector<double2> &hi, std::vector<double2> &lo);
@@ -76,7 +78,17 @@ void build_twiddles(int M, std::vector<double2> &hi, std::vector<double2> &lo);
 // ---------------------------------------------------------------------------
 // Device kernels (s2dw_kernels.cu)
 // ---------------------------------------------------------------------------
-enum CztMode { CZT_ANA_BETA = 0, CZT_ANA_ALPHA = 1, CZT_SYN_ALPHA = 2, CZT_SYN_BETA = 3 };
+// Transform modes.  CZT_* are chirp-z (Bluestein) transforms of any length;
+// FFT_ANA_BETA / FFT_SYN_BETA are the beta transforms as one power-of-two FFT
+// of length 4*bl (used when 4*bl is a power of two).
+enum CztMode {
+    CZT_ANA_BETA = 0,
+    CZT_ANA_ALPHA = 1,
+    CZT_SYN_ALPHA = 2,
+    CZT_SYN_BETA = 3,
+    FFT_ANA_BETA = 4,
+    FFT_SYN_BETA = 5
+};
 
 struct CztDev {
     int M = 0;
@@ -145,6 +157,7 @@ int launch_gprep(const GprepArgs &a, cudaStream_t s);
 int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp, cudaStream_t s);
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
+void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread
 int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
 int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,

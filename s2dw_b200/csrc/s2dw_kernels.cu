@@ -570,193 +570,308 @@ __device__ __forceinline__ double2 twid(const double2 *twh, const double2 *twl, 
     return cmul(twh[x >> 6], twl[x & 63]);
 }
 
-// One Stockham pass of radix R over `rows` transforms of size M held at
-// buf[r*M ...] (padded indices).  Each thread processes NB = 16/R butterflies.
-template <int R, int SIGN>
-__device__ __forceinline__ void fft_pass(double2 *buf, int M, int Ns, int tid,
-                                         const double2 *twh, const double2 *twl)
+// Stockham passes with the data of each pass in registers.  A CTA of T
+// threads holds E = V*T complex values (V per thread): E/M transforms of size
+// M (a power of two).  In a pass of radix R (R <= V) each thread owns V/R
+// butterflies; butterfly (t,u) reads positions r*M + j + s*(M/R) and, after
+// twiddles exp(SIGN 2 pi i (j mod Ns) s/(Ns R)) and a radix-R DFT, writes
+// r*M + (j/Ns)*Ns*R + j%Ns + s*Ns.  The last pass (Ns = M/R) therefore writes
+// exactly the positions the first pass of the same radix reads, so a forward
+// FFT followed by an inverse FFT whose radices run in reverse order keeps the
+// data in registers across the boundary.
+template <int V, int R>
+__device__ __forceinline__ int in_pos(int t, int u, int s, int lgM)
 {
-    constexpr int NB = 16 / R;
-    const int perRow = M / R;
-    double2 v[NB][R];
-    int base[NB], jj[NB];
+    constexpr int NB = V / R, LR = (R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4);
+    const int b = t * NB + u, lper = lgM - LR, r = b >> lper, j = b & ((1 << lper) - 1);
+    return (r << lgM) + j + (s << lper);
+}
+
+template <int V, int R, int SIGN>
+__device__ __forceinline__ void bfly(double2 (&v)[V], int t, int lgM, int lNs, const double2 *twh,
+                                     const double2 *twl)
+{
+    constexpr int NB = V / R, LR = (R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4);
 #pragma unroll
     for (int u = 0; u < NB; u++) {
-        const int b = tid * NB + u, r = b / perRow, j = b % perRow;
-        base[u] = r * M;
-        jj[u] = j;
+        if (lNs > 0) {
+            const int b = t * NB + u, j = b & ((1 << (lgM - LR)) - 1), k = j & ((1 << lNs) - 1);
+            const int step = k << (lgM - lNs - LR);
 #pragma unroll
-        for (int t = 0; t < R; t++) v[u][t] = buf[padix(base[u] + j + t * perRow)];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < NB; u++) {
-        const int j = jj[u], k = j % Ns;
-        const int step = k * (M / (Ns * R));
-#pragma unroll
-        for (int t = 1; t < R; t++) {
-            double2 wv = twid(twh, twl, step * t);
-            if (SIGN > 0) wv = cconj(wv);
-            v[u][t] = cmul(v[u][t], wv);
+            for (int s = 1; s < R; s++) {
+                double2 w = twid(twh, twl, step * s);
+                if (SIGN > 0) w = cconj(w);
+                v[u * R + s] = cmul(v[u * R + s], w);
+            }
         }
-        Dft<R, SIGN>::run(v[u]);
-        const int idx = (j / Ns) * Ns * R + k;
-#pragma unroll
-        for (int t = 0; t < R; t++) buf[padix(base[u] + idx + t * Ns)] = v[u][t];
+        Dft<R, SIGN>::run(&v[u * R]);
     }
-    __syncthreads();
 }
 
-template <int SIGN>
-__device__ void fft_rows(double2 *buf, int M, int tid, const double2 *twh, const double2 *twl)
+template <int V, int R>
+__device__ __forceinline__ void store_pass(const double2 (&v)[V], double2 *buf, int t, int lgM, int lNs)
 {
-    int Ns = 1;
-    while (Ns * 16 <= M) {
-        fft_pass<16, SIGN>(buf, M, Ns, tid, twh, twl);
-        Ns *= 16;
+    constexpr int NB = V / R, LR = (R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4);
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int b = t * NB + u, lper = lgM - LR, r = b >> lper, j = b & ((1 << lper) - 1);
+        const int idx = (r << lgM) + ((j >> lNs) << (lNs + LR)) + (j & ((1 << lNs) - 1));
+#pragma unroll
+        for (int s = 0; s < R; s++) buf[padix(idx + (s << lNs))] = v[u * R + s];
     }
-    const int rem = M / Ns;
-    if (rem == 2) fft_pass<2, SIGN>(buf, M, Ns, tid, twh, twl);
-    else if (rem == 4) fft_pass<4, SIGN>(buf, M, Ns, tid, twh, twl);
-    else if (rem == 8) fft_pass<8, SIGN>(buf, M, Ns, tid, twh, twl);
 }
 
-// rows per CTA so that every CTA holds max(M, 4096) complex values
-__host__ __device__ __forceinline__ int czt_elems(int M) { return M > 4096 ? M : 4096; }
+template <int V, int R>
+__device__ __forceinline__ void load_pass(double2 (&v)[V], const double2 *buf, int t, int lgM)
+{
+    constexpr int NB = V / R;
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+#pragma unroll
+        for (int s = 0; s < R; s++) v[u * R + s] = buf[padix(in_pos<V, R>(t, u, s, lgM))];
+}
 
-__global__ void __launch_bounds__(512) czt_kernel(CztArgs a)
+// Radix plans for M = 2^k: forward [V,...,V,2^(k mod log2 V)], inverse in
+// reverse order.  The radix of pass p is computed, not stored, so that no
+// plan array is indexed dynamically.
+struct RadixPlan {
+    int np, nv, rem;
+    bool rev;
+    __device__ __forceinline__ int r(int p) const
+    {
+        if (rev) return (rem && p == 0) ? (1 << rem) : nv_radix;
+        return (p < nv) ? nv_radix : (1 << rem);
+    }
+    int nv_radix;
+};
+template <int V>
+__device__ __forceinline__ RadixPlan radix_plan(int lgM, bool reversed)
+{
+    constexpr int LV = (V == 8 ? 3 : 4);
+    RadixPlan p;
+    p.nv = lgM / LV;
+    p.rem = lgM % LV;
+    p.np = p.nv + (p.rem ? 1 : 0);
+    p.rev = reversed;
+    p.nv_radix = V;
+    return p;
+}
+
+template <int V, int SIGN>
+__device__ __forceinline__ void bfly_any(double2 (&v)[V], int R, int t, int lgM, int lNs, const double2 *twh,
+                                         const double2 *twl)
+{
+    if (V == 16 && R == 16) bfly<V, (V >= 16 ? 16 : 2), SIGN>(v, t, lgM, lNs, twh, twl);
+    else if (R == 8) bfly<V, 8, SIGN>(v, t, lgM, lNs, twh, twl);
+    else if (R == 4) bfly<V, 4, SIGN>(v, t, lgM, lNs, twh, twl);
+    else bfly<V, 2, SIGN>(v, t, lgM, lNs, twh, twl);
+}
+template <int V>
+__device__ __forceinline__ void store_any(const double2 (&v)[V], int R, double2 *buf, int t, int lgM, int lNs)
+{
+    if (V == 16 && R == 16) store_pass<V, (V >= 16 ? 16 : 2)>(v, buf, t, lgM, lNs);
+    else if (R == 8) store_pass<V, 8>(v, buf, t, lgM, lNs);
+    else if (R == 4) store_pass<V, 4>(v, buf, t, lgM, lNs);
+    else store_pass<V, 2>(v, buf, t, lgM, lNs);
+}
+template <int V>
+__device__ __forceinline__ void load_any(double2 (&v)[V], int R, const double2 *buf, int t, int lgM)
+{
+    if (V == 16 && R == 16) load_pass<V, (V >= 16 ? 16 : 2)>(v, buf, t, lgM);
+    else if (R == 8) load_pass<V, 8>(v, buf, t, lgM);
+    else if (R == 4) load_pass<V, 4>(v, buf, t, lgM);
+    else load_pass<V, 2>(v, buf, t, lgM);
+}
+
+template <int V, int SIGN>
+__device__ __forceinline__ void fft_run(double2 (&v)[V], double2 *buf, int t, int lgM, const RadixPlan &P,
+                                        const double2 *twh, const double2 *twl)
+{
+    int lNs = 0;
+    for (int p = 0; p < P.np; p++) {
+        const int R = P.r(p), LR = 31 - __clz(R);
+        bfly_any<V, SIGN>(v, R, t, lgM, lNs, twh, twl);
+        if (p + 1 < P.np) {
+            store_any<V>(v, R, buf, t, lgM, lNs);
+            __syncthreads();
+            load_any<V>(v, P.r(p + 1), buf, t, lgM);
+            __syncthreads();
+        }
+        lNs += LR;
+    }
+}
+
+// Position (within the CTA buffer) of value i = u*R + s a thread holds for a
+// pass of radix R.
+template <int V>
+__device__ __forceinline__ int pos_of(int i, int R, int t, int lgM)
+{
+    const int LR = 31 - __clz(R), u = i >> LR, s = i & (R - 1);
+    const int b = t * (V / R) + u, lper = lgM - LR, r = b >> lper, j = b & ((1 << lper) - 1);
+    return (r << lgM) + j + (s << lper);
+}
+
+// Input element k of transform `row` of a MODE transform (pre-chirp or
+// pre-twiddle applied); zero outside the transform's input range.
+template <int MODE>
+__device__ __forceinline__ double2 fft_load(const CztArgs &a, int row, int k, const double2 *ph)
+{
+    const int bl = a.bl, n = 2 * bl - 1, N = a.N;
+    const double2 zero = make_double2(0.0, 0.0);
+    if (MODE == CZT_ANA_ALPHA) {  // row = (g, b pair); Hermitian completion in m
+        if (k >= n) return zero;
+        const int g = row / bl, bp = row % bl;
+        const bool lo = k < bl;
+        const double2 *p = a.in_c + ((size_t)g * bl + (lo ? k : n - k)) * (2 * bl) + 2 * bp;
+        double2 x1 = p[0], x2 = p[1];
+        const double2 pr = a.czt.pre[k];
+        if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
+        if (k == 0) { x1.y = 0.0; x2.y = 0.0; }
+        return cmul(make_double2(x1.x - x2.y, x1.y + x2.x), pr);
+    } else if (MODE == CZT_SYN_ALPHA) {  // row = (g, b pair); z = w(:,b1) + i w(:,b2)
+        if (k >= n) return zero;
+        const int g = row / bl, bp = row % bl;
+        const double *p = a.in_r + (size_t)k + (size_t)n * (2 * bp + (size_t)2 * bl * g);
+        return cmul(make_double2(p[0], p[n]), a.czt.pre[k]);
+    } else if (MODE == CZT_ANA_BETA) {  // row = (g, m); k <-> m' = k-(bl-1)
+        if (k >= a.czt.spec.K) return zero;
+        const int g = row / bl, m = row % bl, mpv = k - (bl - 1), ab = mpv < 0 ? -mpv : mpv;
+        double2 x = a.in_c[((size_t)g * bl + m) * bl + ab];
+        if (((m + N - 1) & 1) && mpv < 0) x = make_double2(-x.x, -x.y);
+        return cmul(x, a.czt.pre[k]);
+    } else if (MODE == FFT_ANA_BETA) {  // row = (g, m); k = m' mod 4bl, pre = exp(i pi m'/(4bl))
+        const int g = row / bl, m = row % bl;
+        if (k < bl) return cmul(a.in_c[((size_t)g * bl + m) * bl + k], a.czt.pre[k]);
+        if (k > 3 * bl) {
+            const int p = 4 * bl - k;
+            double2 x = a.in_c[((size_t)g * bl + m) * bl + p];
+            if ((m + N - 1) & 1) x = make_double2(-x.x, -x.y);
+            return cmul(x, cconj(a.czt.pre[p]));
+        }
+        return zero;
+    } else {  // CZT_SYN_BETA / FFT_SYN_BETA: row = (q, m); k = b; gamma DFT on the fly
+        if (k >= 2 * bl) return zero;
+        const int q = row / bl, m = row % bl;
+        double2 u = zero;
+        for (int g = 0; g < N; g++) u = cadd(u, cmul(a.in_c[((size_t)g * bl + m) * (2 * bl) + k], ph[q * N + g]));
+        u = cscale(u, a.wq[k]);
+        return MODE == CZT_SYN_BETA ? cmul(u, a.czt.pre[k]) : u;
+    }
+}
+
+template <int V, int THREADS, int MODE>
+__global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_kernel(CztArgs a)
 {
     extern __shared__ double2 smem[];
-    const int M = a.czt.M, E = czt_elems(M), R = E / M;
+    constexpr int E = V * THREADS;
+    constexpr bool CHIRP = (MODE != FFT_ANA_BETA && MODE != FFT_SYN_BETA);
+    constexpr bool SYNB = (MODE == CZT_SYN_BETA || MODE == FFT_SYN_BETA);
+    const int M = a.czt.M, lgM = 31 - __clz(M), R = E / M;
     double2 *buf = smem;
     double2 *twh = smem + padix(E) + 1;
     const int nhi = (M + 63) / 64;
     double2 *twl = twh + nhi;
-    double2 *ph = twl + 64;  // [q][g] exp(-i pi n_q g / N) for CZT_SYN_BETA
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int bl = a.bl, n = 2 * bl - 1, N = a.N, K = a.czt.spec.K, Bout = a.czt.spec.Bout;
+    double2 *ph = twl + 64;  // [q][g] exp(-i pi n_q g / N) for the synthesis beta modes
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = 2 * bl - 1, N = a.N, Bout = a.czt.spec.Bout;
     const int row0 = blockIdx.x * R;
 
-    for (int i = tid; i < nhi; i += T) twh[i] = a.tw.hi[i];
-    for (int i = tid; i < 64; i += T) twl[i] = a.tw.lo[i];
-    if (a.mode == CZT_SYN_BETA)
-        for (int i = tid; i < a.NP * N; i += T) {
+    for (int i = t; i < nhi; i += THREADS) twh[i] = a.tw.hi[i];
+    for (int i = t; i < 64; i += THREADS) twl[i] = a.tw.lo[i];
+    if (SYNB)
+        for (int i = t; i < a.NP * N; i += THREADS) {
             const int q = i / N, g = i % N;
-            double s, c;
-            sincospi(-(double)(a.nq[q] * g) / (double)N, &s, &c);
-            ph[i] = make_double2(c, s);
+            double sn, cs;
+            sincospi(-(double)(a.nq[q] * g) / (double)N, &sn, &cs);
+            ph[i] = make_double2(cs, sn);
         }
     __syncthreads();
 
-    // ---- load (with pre-chirp), zero padding to M
-    for (int i = tid; i < E; i += T) {
-        const int r = i / M, k = i % M, row = row0 + r;
-        double2 x = make_double2(0.0, 0.0);
-        if (row < a.rows && k < K) {
-            switch (a.mode) {
-            case CZT_ANA_BETA: {  // row = (g, m); k <-> m' = k-(bl-1)
-                const int g = row / bl, m = row % bl, mpv = k - (bl - 1), ab = mpv < 0 ? -mpv : mpv;
-                x = a.in_c[((size_t)g * bl + m) * bl + ab];
-                if (((m + N - 1) & 1) && mpv < 0) x = make_double2(-x.x, -x.y);
-                break;
-            }
-            case CZT_ANA_ALPHA: {  // row = (g, b pair); Hermitian completion in m
-                const int g = row / bl, bp = row % bl;
-                const size_t base = (size_t)g * bl;
-                double2 x1, x2;
-                if (k < bl) {
-                    const double2 *p = a.in_c + (base + k) * (2 * bl) + 2 * bp;
-                    x1 = p[0];
-                    x2 = p[1];
-                    if (k == 0) { x1.y = 0.0; x2.y = 0.0; }
-                } else {
-                    const double2 *p = a.in_c + (base + (n - k)) * (2 * bl) + 2 * bp;
-                    x1 = cconj(p[0]);
-                    x2 = cconj(p[1]);
-                }
-                x = make_double2(x1.x - x2.y, x1.y + x2.x);
-                break;
-            }
-            case CZT_SYN_ALPHA: {  // row = (g, b pair); z = w(:,b1) + i w(:,b2)
-                const int g = row / bl, bp = row % bl;
-                const double *p = a.in_r + (size_t)k + (size_t)n * (2 * bp + (size_t)2 * bl * g);
-                x = make_double2(p[0], p[n]);
-                break;
-            }
-            default: {  // CZT_SYN_BETA: row = (q, m); k = b; gamma DFT on the fly
-                const int q = row / bl, m = row % bl;
-                double2 u = make_double2(0.0, 0.0);
-                for (int g = 0; g < N; g++)
-                    u = cadd(u, cmul(a.in_c[((size_t)g * bl + m) * (2 * bl) + k], ph[q * N + g]));
-                x = cscale(u, a.wq[k]);
-                break;
-            }
-            }
-            x = cmul(x, a.czt.pre[k]);
-        }
-        buf[padix(i)] = x;
-    }
-    __syncthreads();
-    fft_rows<-1>(buf, M, tid, twh, twl);
-    for (int i = tid; i < E; i += T) {
-        const int k = i % M;
-        buf[padix(i)] = cmul(buf[padix(i)], a.czt.Hf[k]);
-    }
-    __syncthreads();
-    fft_rows<+1>(buf, M, tid, twh, twl);
+    const RadixPlan Pf = radix_plan<V>(lgM, false), Pi = radix_plan<V>(lgM, true);
+    const int R0 = (MODE == FFT_ANA_BETA) ? Pi.r(0) : Pf.r(0);
 
-    // ---- post-chirp and store
-    switch (a.mode) {
-    case CZT_ANA_BETA:
-        for (int i = tid; i < R * Bout; i += T) {
-            const int r = i / Bout, b = i % Bout, row = row0 + r;
-            if (row >= a.rows) continue;
-            const int g = row / bl, m = row % bl;
-            a.out_c[((size_t)g * bl + m) * (2 * bl) + b] = cmul(buf[padix(r * M + b)], a.czt.post[b]);
+    double2 v[V];
+#pragma unroll
+    for (int i = 0; i < V; i++) {
+        const int pos = pos_of<V>(i, R0, t, lgM), r = pos >> lgM, k = pos & (M - 1), row = row0 + r;
+        v[i] = (row < a.rows) ? fft_load<MODE>(a, row, k, ph) : make_double2(0.0, 0.0);
+    }
+
+    int RL;  // radix of the last pass run
+    if (MODE == FFT_ANA_BETA) {
+        fft_run<V, +1>(v, buf, t, lgM, Pi, twh, twl);
+        RL = Pi.r(Pi.np - 1);
+    } else if (MODE == FFT_SYN_BETA) {
+        fft_run<V, -1>(v, buf, t, lgM, Pf, twh, twl);
+        RL = Pf.r(Pf.np - 1);
+    } else {
+        fft_run<V, -1>(v, buf, t, lgM, Pf, twh, twl);
+        const int RF = Pf.r(Pf.np - 1);
+#pragma unroll
+        for (int i = 0; i < V; i++) v[i] = cmul(v[i], a.czt.Hf[pos_of<V>(i, RF, t, lgM) & (M - 1)]);
+        fft_run<V, +1>(v, buf, t, lgM, Pi, twh, twl);
+        RL = Pi.r(Pi.np - 1);
+    }
+
+    // ---- store
+    if (MODE == CZT_ANA_BETA || MODE == FFT_ANA_BETA || MODE == CZT_ANA_ALPHA) {
+#pragma unroll
+        for (int i = 0; i < V; i++) {
+            const int pos = pos_of<V>(i, RL, t, lgM), r = pos >> lgM, b = pos & (M - 1), row = row0 + r;
+            if (row >= a.rows || b >= Bout) continue;
+            const double2 y = CHIRP ? cmul(v[i], a.czt.post[b]) : v[i];
+            if (MODE == CZT_ANA_ALPHA) {
+                const int g = row / bl, bp = row % bl;
+                double *p = a.out_r + (size_t)b + (size_t)n * (2 * bp + (size_t)2 * bl * g);
+                p[0] = y.x;
+                p[n] = y.y;
+            } else {
+                const int g = row / bl, m = row % bl;
+                a.out_c[((size_t)g * bl + m) * (2 * bl) + b] = y;
+            }
         }
-        break;
-    case CZT_ANA_ALPHA:
-        for (int i = tid; i < R * Bout; i += T) {
-            const int r = i / Bout, aa = i % Bout, row = row0 + r;
-            if (row >= a.rows) continue;
-            const int g = row / bl, bp = row % bl;
-            const double2 y = cmul(buf[padix(r * M + aa)], a.czt.post[aa]);
-            double *p = a.out_r + (size_t)aa + (size_t)n * (2 * bp + (size_t)2 * bl * g);
-            p[0] = y.x;
-            p[n] = y.y;
-        }
-        break;
-    case CZT_SYN_ALPHA:
-        for (int i = tid; i < R * bl; i += T) {
+        return;
+    }
+    // pair stores go through shared memory
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < V; i++) buf[padix(pos_of<V>(i, RL, t, lgM))] = v[i];
+    __syncthreads();
+    if (MODE == CZT_SYN_ALPHA) {
+        for (int i = t; i < R * bl; i += THREADS) {
             const int r = i / bl, m = i % bl, row = row0 + r;
             if (row >= a.rows) continue;
             const int g = row / bl, bp = row % bl;
             const int mc = (m == 0) ? 0 : n - m;
-            const double2 Z = cmul(buf[padix(r * M + m)], a.czt.post[m]);
-            const double2 Zc = cconj(cmul(buf[padix(r * M + mc)], a.czt.post[mc]));
-            const double2 s = cadd(Z, Zc), d = csub(Z, Zc);
-            const double h = 0.5 * a.scale;
+            const double2 Z = cmul(buf[padix((r << lgM) + m)], a.czt.post[m]);
+            const double2 Zc = cconj(cmul(buf[padix((r << lgM) + mc)], a.czt.post[mc]));
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            const double hh = 0.5 * a.scale;
             double2 *p = a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * bp;
-            p[0] = make_double2(s.x * h, s.y * h);
-            p[1] = make_double2(d.y * h, -d.x * h);
+            p[0] = make_double2(sm.x * hh, sm.y * hh);
+            p[1] = make_double2(d.y * hh, -d.x * hh);
         }
-        break;
-    default:  // CZT_SYN_BETA: fold +-m' and store V2f[q][m][m']
-        for (int i = tid; i < R * bl; i += T) {
-            const int r = i / bl, mpv = i % bl, row = row0 + r;
-            if (row >= a.rows) continue;
-            const int q = row / bl, m = row % bl;
-            const int t0 = bl - 1 + mpv;
-            double2 y = cmul(buf[padix(r * M + t0)], a.czt.post[t0]);
-            if (mpv > 0) {
-                const int t1 = bl - 1 - mpv;
-                double2 z = cmul(buf[padix(r * M + t1)], a.czt.post[t1]);
-                if ((m + a.nq[q]) & 1) z = make_double2(-z.x, -z.y);
-                y = cadd(y, z);
-            }
-            a.out_c[((size_t)q * bl + m) * a.out_stride + mpv] = y;
+        return;
+    }
+    // synthesis beta: V2(m') for m' in (-bl, bl), folded to m' >= 0
+    for (int i = t; i < R * bl; i += THREADS) {
+        const int r = i / bl, mpv = i % bl, row = row0 + r;
+        if (row >= a.rows) continue;
+        const int q = row / bl, m = row % bl;
+        double2 y, z;
+        if (MODE == CZT_SYN_BETA) {
+            const int t0 = bl - 1 + mpv, t1 = bl - 1 - mpv;
+            y = cmul(buf[padix((r << lgM) + t0)], a.czt.post[t0]);
+            z = cmul(buf[padix((r << lgM) + t1)], a.czt.post[t1]);
+        } else {  // V2(m') = exp(-i pi m'/(4bl)) Z(m' mod 4bl)
+            y = cmul(buf[padix((r << lgM) + mpv)], cconj(a.czt.pre[mpv]));
+            z = (mpv > 0) ? cmul(buf[padix((r << lgM) + M - mpv)], a.czt.pre[mpv]) : make_double2(0.0, 0.0);
         }
-        break;
+        if (mpv > 0) {
+            if ((m + a.nq[q]) & 1) z = make_double2(-z.x, -z.y);
+            y = cadd(y, z);
+        }
+        a.out_c[((size_t)q * bl + m) * a.out_stride + mpv] = y;
     }
 }
 
@@ -869,26 +984,54 @@ int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp
     return S2DWC_OK;
 }
 
-int launch_czt(const CztArgs &a, cudaStream_t s)
+template <int V, int THREADS, int MODE>
+static int launch_fft_t(const CztArgs &a, cudaStream_t s)
 {
-    const int M = a.czt.M, E = czt_elems(M), R = E / M;
-    const int threads = E / 16;
+    constexpr int E = V * THREADS;
+    const int M = a.czt.M, R = E / M;
     const int nhi = (M + 63) / 64;
     const size_t smem = sizeof(double2) * ((size_t)padix(E) + 1 + nhi + 64 + 32);
-    static bool attr_set[64] = {false};
+    static bool attr[64] = {false};
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 64 && !attr_set[dev]) {
-        S2DW_CUDA_TRY(cudaFuncSetAttribute(czt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           200 * 1024));
-        attr_set[dev] = true;
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_kernel<V, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(double2) * ((size_t)padix(E) + 1 + 128 + 64 + 32))));
+        attr[dev] = true;
     }
     const int grid = (a.rows + R - 1) / R;
     if (grid == 0) return S2DWC_OK;
-    czt_kernel<<<grid, threads, smem, s>>>(a);
+    fft_kernel<V, THREADS, MODE><<<grid, THREADS, smem, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
+
+template <int V, int THREADS>
+static int launch_fft_mode(const CztArgs &a, cudaStream_t s)
+{
+    switch (a.mode) {
+    case CZT_ANA_BETA: return launch_fft_t<V, THREADS, CZT_ANA_BETA>(a, s);
+    case CZT_ANA_ALPHA: return launch_fft_t<V, THREADS, CZT_ANA_ALPHA>(a, s);
+    case CZT_SYN_ALPHA: return launch_fft_t<V, THREADS, CZT_SYN_ALPHA>(a, s);
+    case CZT_SYN_BETA: return launch_fft_t<V, THREADS, CZT_SYN_BETA>(a, s);
+    case FFT_ANA_BETA: return launch_fft_t<V, THREADS, FFT_ANA_BETA>(a, s);
+    case FFT_SYN_BETA: return launch_fft_t<V, THREADS, FFT_SYN_BETA>(a, s);
+    }
+    return set_error(S2DWC_ERROR_ARG_INVALID, "unknown transform mode %d", a.mode);
+}
+
+static int g_fft_values = 8;  // values per thread of the FFT engine (8 or 16)
+
+int launch_czt(const CztArgs &a, cudaStream_t s)
+{
+    const int M = a.czt.M;
+    if (M < 16 || M > 8192 || (M & (M - 1)))
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "transform size %d unsupported", M);
+    if (g_fft_values == 16) return M <= 4096 ? launch_fft_mode<16, 256>(a, s) : launch_fft_mode<16, 512>(a, s);
+    return M <= 4096 ? launch_fft_mode<8, 512>(a, s) : launch_fft_mode<8, 1024>(a, s);
+}
+
+void set_fft_values(int v) { g_fft_values = (v == 16) ? 16 : 8; }
 
 int launch_zero(double *p, long long n, cudaStream_t s)
 {

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <array>
 #include <cmath>
 #include <complex>
@@ -34,8 +35,9 @@ struct s2dwc_plan {
     double *Om = nullptr, *Acoef = nullptr, *Stm = nullptr, *Gam = nullptr, *Bcoef = nullptr,
            *Em = nullptr, *H = nullptr;
     int32_t *Ste = nullptr, *Ee = nullptr;
-    // per-scale chirp-z tables: [scale][mode]
-    std::vector<std::array<CztDev, 4>> czt;
+    // per-scale transform tables: [scale][CztMode], and the beta modes used
+    std::vector<std::array<CztDev, 6>> czt;
+    std::vector<int> ana_beta_mode, syn_beta_mode;
     std::map<int, TwDev> tw;
     std::vector<double *> wq;  // quadrature weights per scale
     // caller tables folded into per-scale factor tables
@@ -132,13 +134,13 @@ int plan_build(s2dwc_plan *p)
     // chirp-z tables per scale and mode
     p->czt.resize(J + 1);
     p->wq.resize(J + 1);
-    std::map<int, std::array<CztDev, 4>> by_bl;
+    std::map<int, std::array<CztDev, 6>> by_bl;
     std::map<int, double *> wq_by_bl;
     for (int j = 0; j <= J; j++) {
         const int b = p->bl[j], n = 2 * b - 1;
         auto it = by_bl.find(b);
         if (it == by_bl.end()) {
-            std::array<CztDev, 4> arr;
+            std::array<CztDev, 6> arr;
             CztSpec specs[4] = {
                 {2 * b - 1, 2 * b, 4 * b, +1, -2 * (b - 1), 1, 0},  // CZT_ANA_BETA
                 {n, n, n, +1, 0, 0, 0},                              // CZT_ANA_ALPHA
@@ -166,6 +168,27 @@ int plan_build(s2dwc_plan *p)
                     p->tw[c.M] = tw;
                 }
             }
+            const int L4 = 4 * b;
+            if (L4 >= 16 && L4 <= 8192 && (L4 & (L4 - 1)) == 0) {
+                std::vector<double2> tw4;
+                build_beta_twiddles(b, tw4);
+                for (int md : {(int)FFT_ANA_BETA, (int)FFT_SYN_BETA}) {
+                    CztDev d;
+                    d.M = L4;
+                    d.spec = CztSpec{md == FFT_ANA_BETA ? 4 * b : 2 * b, md == FFT_ANA_BETA ? 2 * b : 2 * b - 1,
+                                     L4, md == FFT_ANA_BETA ? 1 : -1, 0, 0, L4};
+                    if ((st = dev_upload(p, &d.pre, tw4))) return st;
+                    arr[md] = d;
+                }
+                if (!p->tw.count(L4)) {
+                    std::vector<double2> hi, lo;
+                    build_twiddles(L4, hi, lo);
+                    TwDev tw;
+                    tw.M = L4;
+                    if ((st = dev_upload(p, &tw.hi, hi)) || (st = dev_upload(p, &tw.lo, lo))) return st;
+                    p->tw[L4] = tw;
+                }
+            }
             it = by_bl.emplace(b, arr).first;
             std::vector<double> w(2 * b);
             for (int bb = 0; bb < 2 * b; bb++)
@@ -176,6 +199,9 @@ int plan_build(s2dwc_plan *p)
         }
         p->czt[j] = it->second;
         p->wq[j] = wq_by_bl[b];
+        const bool fftb = it->second[FFT_ANA_BETA].M > 0;
+        p->ana_beta_mode.push_back(fftb ? FFT_ANA_BETA : CZT_ANA_BETA);
+        p->syn_beta_mode.push_back(fftb ? FFT_SYN_BETA : CZT_SYN_BETA);
     }
     // kernel-table factors
     if ((st = dev_alloc(p, &p->kappaA, (size_t)(J + 1) * B * p->NP)) ||
@@ -307,13 +333,13 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         }
 
         CztArgs ca{};
-        ca.mode = CZT_ANA_BETA;
+        ca.mode = p->ana_beta_mode[j];
         ca.bl = bl;
         ca.N = p->N;
         ca.NP = p->NP;
         std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
         ca.rows = p->N * bl;
-        ca.czt = p->czt[j][CZT_ANA_BETA];
+        ca.czt = p->czt[j][ca.mode];
         ca.tw = p->tw[ca.czt.M];
         ca.in_c = p->wsC;
         ca.out_c = p->wsA;
@@ -365,9 +391,9 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
             if ((st = launch_czt(ca, s))) return st;
         }
 
-        ca.mode = CZT_SYN_BETA;
+        ca.mode = p->syn_beta_mode[j];
         ca.rows = p->NP * bl;
-        ca.czt = p->czt[j][CZT_SYN_BETA];
+        ca.czt = p->czt[j][ca.mode];
         ca.tw = p->tw[ca.czt.M];
         ca.in_c = p->wsA;
         ca.in_r = nullptr;
@@ -459,6 +485,7 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     if (device < 0 || device >= ndev)
         return set_error(S2DWC_ERROR_ARG_INVALID, "device %d out of range (%d devices)", device, ndev);
     DeviceGuard dg(device);
+    if (const char *fv = getenv("S2DW_FFT_VALUES")) set_fft_values(atoi(fv));
     auto *p = new s2dwc_plan();
     p->B = B;
     p->N = N;
