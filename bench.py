@@ -157,6 +157,30 @@ def contraction_flops_per_scale(B, N, alpha, J):
     return ana, syn
 
 
+def fft_flops_per_pair(B, N, alpha, J):
+    """Algorithmic FLOPs of the transform stages per pair, counted as
+    5 L log2 L per complex transform of the length L the stage needs:
+    alpha stages: N*bl complex transforms of length 2bl-1 (two real rows
+    each); beta stages: N*bl (analysis) or ceil(N/2)*bl (synthesis)
+    transforms with 2bl outputs (L = 2bl)."""
+    import math
+
+    from s2dw_b200.core import band_limits
+
+    npos = sum(1 for n in range(N) if (N + n) % 2)
+    out = {"ana_alpha": 0.0, "syn_alpha": 0.0, "ana_beta": 0.0, "syn_beta": 0.0}
+    for j in range(J + 1):
+        bl, _ = band_limits(j, B, alpha)
+        n = 2 * bl - 1
+        fa = 5.0 * n * math.log2(max(n, 2))
+        fb = 5.0 * (2 * bl) * math.log2(2 * bl)
+        out["ana_alpha"] += N * bl * fa
+        out["syn_alpha"] += N * bl * fa
+        out["ana_beta"] += N * bl * fb
+        out["syn_beta"] += npos * bl * fb
+    return out
+
+
 def measured_fp64_peak():
     """FP64 reference rate on this GPU: best of 10 torch.matmul float64 4096^3
     (cuBLAS DGEMM), TFLOP/s."""
@@ -278,8 +302,6 @@ def main():
     recon = float(np.abs(d_out.cpu().numpy().T - flms[(args.warmup - 1) % nring]).max())
 
     clocks = ClockSampler(local)
-    plan.set_timing(True)
-    plan.timing(reset=True)
     barrier(world)
     torch.cuda.synchronize()
     clocks.start()
@@ -291,35 +313,44 @@ def main():
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
-    plan.set_timing(False)
     elapsed = e0.elapsed_time(e1) / 1e3
     elapsed = max_over_ranks(elapsed, world)
-    kt = plan.timing(reset=True)
     pairs = args.steps * world
     value = pairs / elapsed
     la, ls = plan.launch_counts()
+
+    # ---- per-kernel device times: a second timed loop in which the plan
+    # brackets every launch with CUDA events (scales serialised on `stream`)
+    ksteps = max(3, min(args.steps, 10))
+    plan.set_timing(True)
+    plan.timing(reset=True)
+    for i in range(ksteps):
+        step(i)
+    torch.cuda.synchronize()
+    kt = plan.timing(reset=True)
+    plan.set_timing(False)
 
     # ---- roofline of the dominant kernel (largest device-time share)
     fp64_peak = measured_fp64_peak()
     ana_f, syn_f = contraction_flops_per_scale(B, N, alpha, J)
     dom = max(kt.items(), key=lambda kv: kv[1][1])
+    algo = dict(fft_flops_per_pair(B, N, alpha, J))
+    algo["lwalk"], algo["mwalk"] = sum(ana_f), sum(syn_f)
+    n_launch, ms = dom[1]
     roofline = None
-    if dom[0] in ("lwalk", "mwalk"):
-        flops_per_pair = sum(ana_f) if dom[0] == "lwalk" else sum(syn_f)
-        n_launch, ms = dom[1]
+    if dom[0] in algo and n_launch:
         per_launch_ms = ms / n_launch
-        launches_per_pair = n_launch / args.steps
-        achieved = flops_per_pair / launches_per_pair / (per_launch_ms / 1e3) / 1e12
+        launches_per_pair = n_launch / ksteps
+        achieved = algo[dom[0]] / launches_per_pair / (per_launch_ms / 1e3) / 1e12
         roofline = {"kernel": dom[0], "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
                     "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                    "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (fp64 has no entry in MEASURED_PEAKS.json)"}
-    else:
-        n_launch, ms = dom[1]
-        roofline = {"kernel": dom[0], "bound": "fp64", "achieved": None, "peak": fp64_peak,
-                    "unit": "TFLOP/s", "frac": None, "traffic": None,
-                    "note": "dominant kernel is a transform stage"}
-    kernel_ms = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps}
-                 for k, v in kt.items()}
+                    "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (MEASURED_PEAKS.json has no fp64 entry)",
+                    "flops_per_pair": algo[dom[0]], "launches_per_pair": launches_per_pair,
+                    "avg_launch_ms": per_launch_ms}
+    kernel_tflops = {k: (algo[k] * ksteps / (v[1] / 1e3) / 1e12 if k in algo and v[1] > 0 else None)
+                     for k, v in kt.items()}
+    kernel_ms = {k: {"launches_per_step": v[0] / ksteps, "ms_per_step": v[1] / ksteps,
+                     "tflops": kernel_tflops[k]} for k, v in kt.items()}
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None

@@ -175,10 +175,12 @@ int s2dwc_plan_synthesis(s2dwc_plan *plan, double *d_flm, const double *d_wav,
 /* Number of CUDA kernels one analysis / one synthesis launches. */
 int s2dwc_plan_launch_count(const s2dwc_plan *plan, int *analysis, int *synthesis);
 
-/* Per-kernel timing.  When enabled, every launch of the plan is bracketed by
- * CUDA events on its stream; s2dwc_plan_timing() resolves the events
- * (synchronising on them) and returns, for one kernel kind, the launches
- * and total device milliseconds accumulated since the last reset. */
+/* Per-kernel timing.  When enabled, the scales run one after another on the
+ * caller's stream (instead of concurrently on the plan's streams) and every
+ * launch is bracketed by CUDA events on that stream; s2dwc_plan_timing()
+ * resolves the events (synchronising on them) and returns, for one kernel
+ * kind, the launches and total device milliseconds accumulated since the
+ * last reset. */
 #define S2DWC_KIND_LWALK 0     /* analysis contraction + gamma DFT */
 #define S2DWC_KIND_MWALK 1     /* synthesis contraction + harmonic sum */
 #define S2DWC_KIND_ANA_BETA 2  /* analysis beta transform */

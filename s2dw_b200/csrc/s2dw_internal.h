@@ -125,7 +125,19 @@ struct MwalkArgs {
     int Gs;               // roundup(bl, 8)
     const double2 *V2f;   // [(q*bl + m)*Vs + m']
     int Vs;               // roundup(bl, 8)
-    double2 *flm;         // (B,B) column-major, accumulated
+    double2 *part;        // this scale's flm contribution [(l-blo-1)*bl + m], m <= l
+};
+
+// flm(l,m) = sum_j part_j(l,m) + Phi2(l) scoeff(l,m), the scale sum of
+// s2dw_core_mod.f90:1228-1253 in scale order followed by :1258-1261.
+struct CombineArgs {
+    int B, J, bs;
+    int bl[16], blo[16];
+    long long off[16];   // offset of part_j in `parts` (complex values)
+    const double2 *parts;
+    const double2 *scoeff;
+    const double *Phi2;
+    double2 *flm;
 };
 
 // Per-scale factor tables G (see LwalkArgs / MwalkArgs), built at
@@ -162,5 +174,6 @@ int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
 int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,
                        cudaStream_t s);
+int launch_combine(const CombineArgs &a, cudaStream_t s);
 
 }  // namespace s2dw

@@ -507,14 +507,13 @@ __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles
         }
         __syncthreads();
     }
-    // flm(l,m) += i^m * acc (the eta and i^{-n} phases are folded into G)
+    // this scale's flm(l,m) = i^m * acc (the eta and i^{-n} phases are folded into G)
     const double sc = ldexp(1.0, -Kw);
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         if (!val[q]) continue;
         const int m = mbase + w * Q + q;
-        double2 *f = a.flm + (size_t)l + (size_t)B * m;
-        *f = cadd(*f, cipow(cscale(acc[q], sc), m));
+        a.part[(size_t)(l - blo - 1) * bl + m] = cipow(cscale(acc[q], sc), m);
     }
 }
 
@@ -902,6 +901,22 @@ __global__ void scaling_add_kernel(double2 *flm, const double2 *sc, const double
     }
 }
 
+__global__ void combine_kernel(CombineArgs a)
+{
+    const int B = a.B;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)B * B;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(i % B), m = (int)(i / B);
+        double2 f = make_double2(0.0, 0.0);
+        if (m <= l) {
+            for (int j = 0; j <= a.J; j++)
+                if (l > a.blo[j] && l < a.bl[j]) f = cadd(f, a.parts[a.off[j] + (size_t)(l - a.blo[j] - 1) * a.bl[j] + m]);
+        }
+        if (l < a.bs && m < a.bs) f = cadd(f, cscale(a.scoeff[l + (size_t)a.bs * m], a.Phi2[l]));
+        a.flm[i] = f;
+    }
+}
+
 // ===========================================================================
 // Launchers
 // ===========================================================================
@@ -1032,6 +1047,15 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
 }
 
 void set_fft_values(int v) { g_fft_values = (v == 16) ? 16 : 8; }
+
+int launch_combine(const CombineArgs &a, cudaStream_t s)
+{
+    long long n = (long long)a.B * a.B, blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    combine_kernel<<<(int)blocks, 256, 0, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
 
 int launch_zero(double *p, long long n, cudaStream_t s)
 {

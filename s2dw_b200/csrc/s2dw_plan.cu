@@ -46,8 +46,14 @@ struct s2dwc_plan {
     std::vector<long long> ga_off, gs_off;       // per-scale offsets (doubles)
     std::vector<int> ga_stride, gs_stride;
     double2 *Fw = nullptr;                       // per-call F table [l*Bp + m]
-    // workspaces
-    double2 *wsA = nullptr, *wsC = nullptr;
+    // per-scale workspaces (scales run concurrently on their own streams):
+    // A_j holds Tb / V (N x bl x 2bl), C_j holds Tg (N x bl x bl) / V2f,
+    // P_j the scale's flm rows (bl-blo-1) x bl
+    double2 *wsA = nullptr, *wsC = nullptr, *wsP = nullptr;
+    std::vector<long long> offA, offC, offP;
+    std::vector<cudaStream_t> streams;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_join;
     // device buffers of the host-buffer entry points (allocated on first use)
     double *hbWav = nullptr;
     double2 *hbFlm = nullptr, *hbSc = nullptr;
@@ -70,6 +76,9 @@ struct s2dwc_plan {
             cudaEventDestroy(std::get<1>(t));
             cudaEventDestroy(std::get<2>(t));
         }
+        for (auto st : streams) cudaStreamDestroy(st);
+        for (auto ev : ev_join) cudaEventDestroy(ev);
+        if (ev_fork) cudaEventDestroy(ev_fork);
         for (void *p : allocs) cudaFree(p);
         cudaSetDevice(cur);
     }
@@ -223,11 +232,27 @@ int plan_build(s2dwc_plan *p)
         (st = dev_alloc(p, &p->Gsyn, (size_t)std::max(1LL, ns))) ||
         (st = dev_alloc(p, &p->Fw, (size_t)B * Bp)))
         return st;
-    // workspaces: wsA holds Tb / V (N x bl x 2bl), wsC holds Tg (N x bl x bl)
-    // and V2f (NP x bl x roundup(bl,8))
-    const size_t nA = (size_t)N * B * 2 * B;
-    const size_t nC = std::max((size_t)N * B * B, (size_t)p->NP * B * ((B + 7) / 8 * 8));
-    if ((st = dev_alloc(p, &p->wsA, nA)) || (st = dev_alloc(p, &p->wsC, nC))) return st;
+    // per-scale workspaces
+    long long nA = 0, nC = 0, nP = 0;
+    for (int j = 0; j <= J; j++) {
+        const long long b = p->bl[j];
+        p->offA.push_back(nA);
+        p->offC.push_back(nC);
+        p->offP.push_back(nP);
+        nA += (long long)N * b * 2 * b;
+        nC += std::max((long long)N * b * b, (long long)p->NP * b * p->gs_stride[j]);
+        nP += (long long)std::max(0, p->bl[j] - p->blo[j] - 1) * b;
+    }
+    if ((st = dev_alloc(p, &p->wsA, (size_t)nA)) || (st = dev_alloc(p, &p->wsC, (size_t)nC)) ||
+        (st = dev_alloc(p, &p->wsP, (size_t)std::max(1LL, nP))))
+        return st;
+    p->streams.resize(J + 1);
+    p->ev_join.resize(J + 1);
+    for (int j = 0; j <= J; j++) {
+        S2DW_CUDA_TRY(cudaStreamCreateWithFlags(&p->streams[j], cudaStreamNonBlocking));
+        S2DW_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_join[j], cudaEventDisableTiming));
+    }
+    S2DW_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
     return S2DWC_OK;
 }
 
@@ -242,6 +267,7 @@ int validate_sizes(int B, int N, double alpha, int J)
     if (N > B) return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d exceeds B=%d", N, B);
     if (!(alpha > 1.0)) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha=%g must exceed 1", alpha);
     if (B > 2048) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d exceeds the supported 2048", B);
+    if (J > 15) return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d exceeds the supported 15", J);
     if (!params_valid(J, B, alpha, N))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d invalid for B=%d alpha=%g (1<=J<=%d)", J, B,
                          alpha, comp_jmax(B, alpha));
@@ -302,7 +328,8 @@ struct KernelTimer {
     }
 };
 
-// Runs the analysis of every scale on `s`.
+// Runs the analysis: the F table on `s`, then every scale on its own stream
+// (forked from and joined back to `s`).
 int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s)
 {
     int st;
@@ -310,8 +337,14 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         KernelTimer kt(p, S2DWC_KIND_OTHER, s);
         if ((st = launch_fprep(p->Fw, d_flm, p->Om, p->B, p->Bp, s))) return st;
     }
+    S2DW_CUDA_TRY(cudaEventRecord(p->ev_fork, s));
     for (int j = 0; j <= p->J; j++) {
+        // per-kernel timing runs every launch on the caller's stream so that
+        // each event pair brackets one kernel running alone
+        cudaStream_t sj = p->timing ? s : p->streams[j];
+        if (!p->timing) S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_fork, 0));
         const int bl = p->bl[j];
+        double2 *Tg = p->wsC + p->offC[j], *Tb = p->wsA + p->offA[j];
         LwalkArgs la{};
         la.B = p->B;
         la.Bp = p->Bp;
@@ -326,12 +359,11 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         la.G = p->Ga + p->ga_off[j];
         la.Gs = p->ga_stride[j];
         la.F = p->Fw;
-        la.Tg = p->wsC;
+        la.Tg = Tg;
         {
-            KernelTimer kt(p, S2DWC_KIND_LWALK, s);
-            if ((st = launch_lwalk(la, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
+            if ((st = launch_lwalk(la, sj))) return st;
         }
-
         CztArgs ca{};
         ca.mode = p->ana_beta_mode[j];
         ca.bl = bl;
@@ -341,39 +373,44 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         ca.rows = p->N * bl;
         ca.czt = p->czt[j][ca.mode];
         ca.tw = p->tw[ca.czt.M];
-        ca.in_c = p->wsC;
-        ca.out_c = p->wsA;
+        ca.in_c = Tg;
+        ca.out_c = Tb;
         {
-            KernelTimer kt(p, S2DWC_KIND_ANA_BETA, s);
-            if ((st = launch_czt(ca, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_ANA_BETA, sj);
+            if ((st = launch_czt(ca, sj))) return st;
         }
-
         ca.mode = CZT_ANA_ALPHA;
         ca.rows = p->N * bl;  // (g, b pair)
         ca.czt = p->czt[j][CZT_ANA_ALPHA];
         ca.tw = p->tw[ca.czt.M];
-        ca.in_c = p->wsA;
+        ca.in_c = Tb;
         ca.out_c = nullptr;
         ca.out_r = d_wav + p->wav_off[j];
         {
-            KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, s);
-            if ((st = launch_czt(ca, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, sj);
+            if ((st = launch_czt(ca, sj))) return st;
         }
+        if (!p->timing) S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], sj));
     }
-    KernelTimer kt(p, S2DWC_KIND_OTHER, s);
-    return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
+    {
+        KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+        if ((st = launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s))) return st;
+    }
+    if (p->timing) return S2DWC_OK;
+    for (int j = 0; j <= p->J; j++) S2DW_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[j], 0));
+    return S2DWC_OK;
 }
 
 int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const double2 *d_scoeff,
                   cudaStream_t s)
 {
     int st;
-    {
-        KernelTimer kt(p, S2DWC_KIND_OTHER, s);
-        if ((st = launch_zero(reinterpret_cast<double *>(d_flm), 2LL * p->B * p->B, s))) return st;
-    }
+    S2DW_CUDA_TRY(cudaEventRecord(p->ev_fork, s));
     for (int j = 0; j <= p->J; j++) {
+        cudaStream_t sj = p->timing ? s : p->streams[j];
+        if (!p->timing) S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_fork, 0));
         const int bl = p->bl[j];
+        double2 *Vw = p->wsA + p->offA[j], *V2f = p->wsC + p->offC[j];
         CztArgs ca{};
         ca.mode = CZT_SYN_ALPHA;
         ca.bl = bl;
@@ -384,27 +421,25 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ca.czt = p->czt[j][CZT_SYN_ALPHA];
         ca.tw = p->tw[ca.czt.M];
         ca.in_r = d_wav + p->wav_off[j];
-        ca.out_c = p->wsA;
+        ca.out_c = Vw;
         ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
         {
-            KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, s);
-            if ((st = launch_czt(ca, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, sj);
+            if ((st = launch_czt(ca, sj))) return st;
         }
-
         ca.mode = p->syn_beta_mode[j];
         ca.rows = p->NP * bl;
         ca.czt = p->czt[j][ca.mode];
         ca.tw = p->tw[ca.czt.M];
-        ca.in_c = p->wsA;
+        ca.in_c = Vw;
         ca.in_r = nullptr;
-        ca.out_c = p->wsC;
+        ca.out_c = V2f;
         ca.out_stride = p->gs_stride[j];
         ca.wq = p->wq[j];
         {
-            KernelTimer kt(p, S2DWC_KIND_SYN_BETA, s);
-            if ((st = launch_czt(ca, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_SYN_BETA, sj);
+            if ((st = launch_czt(ca, sj))) return st;
         }
-
         MwalkArgs ma{};
         ma.B = p->B;
         ma.Bp = p->Bp;
@@ -418,16 +453,32 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ma.Ee = p->Ee;
         ma.G = p->Gsyn + p->gs_off[j];
         ma.Gs = p->gs_stride[j];
-        ma.V2f = p->wsC;
+        ma.V2f = V2f;
         ma.Vs = p->gs_stride[j];
-        ma.flm = d_flm;
+        ma.part = p->wsP + p->offP[j];
         {
-            KernelTimer kt(p, S2DWC_KIND_MWALK, s);
-            if ((st = launch_mwalk(ma, s))) return st;
+            KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
+            if ((st = launch_mwalk(ma, sj))) return st;
         }
+        if (!p->timing) S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], sj));
     }
+    if (!p->timing)
+        for (int j = 0; j <= p->J; j++) S2DW_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[j], 0));
+    CombineArgs cb{};
+    cb.B = p->B;
+    cb.J = p->J;
+    cb.bs = p->bl_scoeff;
+    for (int j = 0; j <= p->J; j++) {
+        cb.bl[j] = p->bl[j];
+        cb.blo[j] = p->blo[j];
+        cb.off[j] = p->offP[j];
+    }
+    cb.parts = p->wsP;
+    cb.scoeff = d_scoeff;
+    cb.Phi2 = p->Phi2;
+    cb.flm = d_flm;
     KernelTimer kt(p, S2DWC_KIND_OTHER, s);
-    return launch_scaling_add(d_flm, d_scoeff, p->Phi2, p->B, p->bl_scoeff, s);
+    return launch_combine(cb, s);
 }
 
 }  // namespace
@@ -594,7 +645,7 @@ int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
 {
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "launch_count: null plan");
     if (analysis) *analysis = 3 * (p->J + 1) + 2;
-    int ns = 2;
+    int ns = 1;
     for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? 1 : 0);
     if (synthesis) *synthesis = ns;
     return S2DWC_OK;
