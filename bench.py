@@ -47,40 +47,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_setup():
-    import torch
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return world, rank, local
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-
-
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -274,8 +240,11 @@ def main():
     from s2dw_b200.device import Plan
     from s2dw_b200.workload import gaussian_flm, transform_setup
 
-    world, rank, local = dist_setup()
+    from s2dw_b200 import replicas
+
+    world, rank, local = replicas.init_group("nccl")
     torch.cuda.set_device(local)
+    barrier, max_over_ranks = replicas.barrier, replicas.max_over_ranks
     B, N, alpha = args.B, args.N, args.alpha
     t = transform_setup(B, N, alpha)
     J = t["J"]
@@ -420,10 +389,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     plan.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 if __name__ == "__main__":
