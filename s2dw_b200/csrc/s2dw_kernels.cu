@@ -875,6 +875,271 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
 }
 
 // ===========================================================================
+// Large transforms (M = 4096, 8192): one transform per CTA, compile-time size
+//
+// Radix-16 Stockham passes with 16 values per thread (THREADS = M/16), the
+// shape with the fewest shared-memory exchanges.  The twiddles of a pass are
+// the powers w^s (s = 1..15) of one root w = W_M^step: w from the two-level
+// table, w^2..w^15 by products (w^8 and w^4 squarings, then products), which
+// keeps shared-memory traffic to the data exchanges.  The row (g, m) or
+// (g, b pair) comes from the 2-D grid, so no integer division is needed.
+// ===========================================================================
+template <int SIGN>
+__device__ __forceinline__ void twiddle_powers16(double2 (&v)[16], double2 w)
+{
+    if (SIGN > 0) w = cconj(w);
+    const double2 w2 = cmul(w, w), w4 = cmul(w2, w2), w8 = cmul(w4, w4);
+    const double2 w3 = cmul(w2, w), w5 = cmul(w4, w), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+    v[1] = cmul(v[1], w);
+    v[2] = cmul(v[2], w2);
+    v[3] = cmul(v[3], w3);
+    v[4] = cmul(v[4], w4);
+    v[5] = cmul(v[5], w5);
+    v[6] = cmul(v[6], w6);
+    v[7] = cmul(v[7], w7);
+    v[8] = cmul(v[8], w8);
+    v[9] = cmul(v[9], cmul(w8, w));
+    v[10] = cmul(v[10], cmul(w8, w2));
+    v[11] = cmul(v[11], cmul(w8, w3));
+    v[12] = cmul(v[12], cmul(w8, w4));
+    v[13] = cmul(v[13], cmul(w8, w5));
+    v[14] = cmul(v[14], cmul(w8, w6));
+    v[15] = cmul(v[15], cmul(w8, w7));
+}
+
+// One radix-16 pass (16 values per thread, thread t = butterfly j).
+template <int LGM, int LNS, int SIGN>
+__device__ __forceinline__ void pass16(double2 (&v)[16], int t, const double2 *twh, const double2 *twl)
+{
+    if (LNS > 0) {
+        const int k = t & ((1 << LNS) - 1);
+        twiddle_powers16<SIGN>(v, twid(twh, twl, k << (LGM - LNS - 4)));
+    }
+    Dft<16, SIGN>::run(v);
+}
+
+// Radix-2 pass for LGM = 13 (the remainder of 13 = 4+4+4+1), 8 butterflies per thread.
+template <int LGM, int LNS, int SIGN>
+__device__ __forceinline__ void pass2x8(double2 (&v)[16], int t, const double2 *twh, const double2 *twl)
+{
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        if (LNS > 0) {
+            const int j = (t * 8 + u) & ((1 << (LGM - 1)) - 1), k = j & ((1 << LNS) - 1);
+            double2 w = twid(twh, twl, k << (LGM - LNS - 1));
+            if (SIGN > 0) w = cconj(w);
+            v[2 * u + 1] = cmul(v[2 * u + 1], w);
+        }
+        const double2 a = v[2 * u], b = v[2 * u + 1];
+        v[2 * u] = cadd(a, b);
+        v[2 * u + 1] = csub(a, b);
+    }
+}
+
+// Shared-memory exchange after a pass of radix R at LNS into the input
+// positions of the next pass of radix RN (values per thread: 16).
+template <int LGM, int R, int LNS, int RN>
+__device__ __forceinline__ void exchange(double2 (&v)[16], double2 *buf, int t)
+{
+    constexpr int NB = 16 / R, LR = (R == 16 ? 4 : 1), NBN = 16 / RN, LRN = (RN == 16 ? 4 : 1);
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int j = t * NB + u;
+        const int idx = ((j >> LNS) << (LNS + LR)) + (j & ((1 << LNS) - 1));
+#pragma unroll
+        for (int s = 0; s < R; s++) buf[padix(idx + (s << LNS))] = v[u * R + s];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < NBN; u++) {
+        const int j = t * NBN + u;
+#pragma unroll
+        for (int s = 0; s < RN; s++) v[u * RN + s] = buf[padix(j + (s << (LGM - LRN)))];
+    }
+    __syncthreads();
+}
+
+// Forward (SIGN=-1, radices 16,16,16[,2]) or inverse (SIGN=+1, [2,]16,16,16)
+// FFT of the values in registers; input positions of the first pass, output
+// positions of the last pass.
+template <int LGM, int SIGN>
+__device__ __forceinline__ void fft_large(double2 (&v)[16], double2 *buf, int t, const double2 *twh,
+                                          const double2 *twl)
+{
+    if (LGM == 12) {
+        pass16<12, 0, SIGN>(v, t, twh, twl);
+        exchange<12, 16, 0, 16>(v, buf, t);
+        pass16<12, 4, SIGN>(v, t, twh, twl);
+        exchange<12, 16, 4, 16>(v, buf, t);
+        pass16<12, 8, SIGN>(v, t, twh, twl);
+    } else if (SIGN < 0) {  // LGM == 13 forward: 16,16,16,2
+        pass16<13, 0, SIGN>(v, t, twh, twl);
+        exchange<13, 16, 0, 16>(v, buf, t);
+        pass16<13, 4, SIGN>(v, t, twh, twl);
+        exchange<13, 16, 4, 16>(v, buf, t);
+        pass16<13, 8, SIGN>(v, t, twh, twl);
+        exchange<13, 16, 8, 2>(v, buf, t);
+        pass2x8<13, 12, SIGN>(v, t, twh, twl);
+    } else {  // LGM == 13 inverse: 2,16,16,16
+        pass2x8<13, 0, SIGN>(v, t, twh, twl);
+        exchange<13, 2, 0, 16>(v, buf, t);
+        pass16<13, 1, SIGN>(v, t, twh, twl);
+        exchange<13, 16, 1, 16>(v, buf, t);
+        pass16<13, 5, SIGN>(v, t, twh, twl);
+        exchange<13, 16, 5, 16>(v, buf, t);
+        pass16<13, 9, SIGN>(v, t, twh, twl);
+    }
+}
+
+// Position in [0, M) of value i held by thread t at the input of a pass of
+// radix R (R = 16: i = s; R = 2: i = 2u + s).
+template <int LGM, int R>
+__device__ __forceinline__ int lpos(int t, int i)
+{
+    if (R == 16) return t + (i << (LGM - 4));
+    const int u = i >> 1, s = i & 1;
+    return ((t * 8 + u) & ((1 << (LGM - 1)) - 1)) + (s << (LGM - 1));
+}
+
+template <int MODE, int LGM>
+__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_large_kernel(CztArgs a)
+{
+    constexpr int M = 1 << LGM, THREADS = M / 16;
+    constexpr bool CHIRP = (MODE != FFT_ANA_BETA && MODE != FFT_SYN_BETA);
+    constexpr bool SYNB = (MODE == CZT_SYN_BETA || MODE == FFT_SYN_BETA);
+    // first-pass radix of the transform run first, last-pass radix of the last
+    constexpr int R0 = (LGM == 13 && MODE == FFT_ANA_BETA) ? 2 : 16;
+    constexpr int RL = (LGM == 13 && MODE == FFT_SYN_BETA) ? 2 : 16;
+    extern __shared__ double2 smem[];
+    double2 *buf = smem;
+    double2 *twh = smem + padix(M) + 1;
+    double2 *twl = twh + M / 64;
+    double2 *ph = twl + 64;
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = 2 * bl - 1, N = a.N, Bout = a.czt.spec.Bout;
+    const int g = blockIdx.y, rr = blockIdx.x;  // row = (g or q, m or b pair)
+    const double2 zero = make_double2(0.0, 0.0);
+
+    for (int i = t; i < M / 64; i += THREADS) twh[i] = a.tw.hi[i];
+    for (int i = t; i < 64; i += THREADS) twl[i] = a.tw.lo[i];
+    if (SYNB && t < N) {
+        double sn, cs;
+        sincospi(-(double)(a.nq[g] * t) / (double)N, &sn, &cs);
+        ph[t] = make_double2(cs, sn);
+    }
+    __syncthreads();
+
+    double2 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int k = lpos<LGM, R0>(t, i);
+        double2 x = zero;
+        if (MODE == CZT_ANA_ALPHA) {  // (g, b pair rr); Hermitian completion in m
+            if (k < n) {
+                const bool lo = k < bl;
+                const double2 *p = a.in_c + ((size_t)g * bl + (lo ? k : n - k)) * (2 * bl) + 2 * rr;
+                double2 x1 = p[0], x2 = p[1];
+                if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
+                if (k == 0) { x1.y = 0.0; x2.y = 0.0; }
+                x = cmul(make_double2(x1.x - x2.y, x1.y + x2.x), a.czt.pre[k]);
+            }
+        } else if (MODE == CZT_SYN_ALPHA) {  // (g, b pair rr)
+            if (k < n) {
+                const double *p = a.in_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+                x = cmul(make_double2(p[0], p[n]), a.czt.pre[k]);
+            }
+        } else if (MODE == CZT_ANA_BETA) {  // (g, m = rr)
+            if (k < a.czt.spec.K) {
+                const int mpv = k - (bl - 1), ab = mpv < 0 ? -mpv : mpv;
+                x = a.in_c[((size_t)g * bl + rr) * bl + ab];
+                if (((rr + N - 1) & 1) && mpv < 0) x = make_double2(-x.x, -x.y);
+                x = cmul(x, a.czt.pre[k]);
+            }
+        } else if (MODE == FFT_ANA_BETA) {  // (g, m = rr), k = m' mod 4bl
+            if (k < bl) {
+                x = cmul(a.in_c[((size_t)g * bl + rr) * bl + k], a.czt.pre[k]);
+            } else if (k > 3 * bl) {
+                const int pp = 4 * bl - k;
+                x = a.in_c[((size_t)g * bl + rr) * bl + pp];
+                if ((rr + N - 1) & 1) x = make_double2(-x.x, -x.y);
+                x = cmul(x, cconj(a.czt.pre[pp]));
+            }
+        } else {  // synthesis beta, (q = g, m = rr), k = b
+            if (k < 2 * bl) {
+                double2 u = zero;
+                for (int gg = 0; gg < N; gg++)
+                    u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + k], ph[gg]));
+                x = cscale(u, a.wq[k]);
+                if (MODE == CZT_SYN_BETA) x = cmul(x, a.czt.pre[k]);
+            }
+        }
+        v[i] = x;
+    }
+
+    if (MODE == FFT_ANA_BETA) {
+        fft_large<LGM, +1>(v, buf, t, twh, twl);
+    } else if (MODE == FFT_SYN_BETA) {
+        fft_large<LGM, -1>(v, buf, t, twh, twl);
+    } else {
+        fft_large<LGM, -1>(v, buf, t, twh, twl);
+        constexpr int RF = (LGM == 13) ? 2 : 16;
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], a.czt.Hf[lpos<LGM, RF>(t, i)]);
+        fft_large<LGM, +1>(v, buf, t, twh, twl);
+    }
+
+    if (MODE == CZT_ANA_BETA || MODE == FFT_ANA_BETA || MODE == CZT_ANA_ALPHA) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int b = lpos<LGM, RL>(t, i);
+            if (b >= Bout) continue;
+            const double2 y = CHIRP ? cmul(v[i], a.czt.post[b]) : v[i];
+            if (MODE == CZT_ANA_ALPHA) {
+                double *p = a.out_r + (size_t)b + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+                p[0] = y.x;
+                p[n] = y.y;
+            } else {
+                a.out_c[((size_t)g * bl + rr) * (2 * bl) + b] = y;
+            }
+        }
+        return;
+    }
+    // pair stores through shared memory
+#pragma unroll
+    for (int i = 0; i < 16; i++) buf[padix(lpos<LGM, RL>(t, i))] = v[i];
+    __syncthreads();
+    if (MODE == CZT_SYN_ALPHA) {
+        for (int m = t; m < bl; m += THREADS) {
+            const int mc = (m == 0) ? 0 : n - m;
+            const double2 Z = cmul(buf[padix(m)], a.czt.post[m]);
+            const double2 Zc = cconj(cmul(buf[padix(mc)], a.czt.post[mc]));
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            const double hh = 0.5 * a.scale;
+            double2 *p = a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr;
+            p[0] = make_double2(sm.x * hh, sm.y * hh);
+            p[1] = make_double2(d.y * hh, -d.x * hh);
+        }
+        return;
+    }
+    for (int mpv = t; mpv < bl; mpv += THREADS) {
+        double2 y, z;
+        if (MODE == CZT_SYN_BETA) {
+            const int t0 = bl - 1 + mpv, t1 = bl - 1 - mpv;
+            y = cmul(buf[padix(t0)], a.czt.post[t0]);
+            z = cmul(buf[padix(t1)], a.czt.post[t1]);
+        } else {
+            y = cmul(buf[padix(mpv)], cconj(a.czt.pre[mpv]));
+            z = (mpv > 0) ? cmul(buf[padix(M - mpv)], a.czt.pre[mpv]) : zero;
+        }
+        if (mpv > 0) {
+            if ((rr + a.nq[g]) & 1) z = make_double2(-z.x, -z.y);
+            y = cadd(y, z);
+        }
+        a.out_c[((size_t)g * bl + rr) * a.out_stride + mpv] = y;
+    }
+}
+
+// ===========================================================================
 // Small kernels
 // ===========================================================================
 __global__ void zero_kernel(double *p, long long n)
@@ -1035,18 +1300,57 @@ static int launch_fft_mode(const CztArgs &a, cudaStream_t s)
     return set_error(S2DWC_ERROR_ARG_INVALID, "unknown transform mode %d", a.mode);
 }
 
-static int g_fft_values = 8;  // values per thread of the FFT engine (8 or 16)
+template <int MODE, int LGM>
+static int launch_large_t(const CztArgs &a, cudaStream_t s)
+{
+    constexpr int M = 1 << LGM;
+    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + 8);
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_large_kernel<MODE, LGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        attr[dev] = true;
+    }
+    // rows are (g or q) x (m or b pair); every mode has bl rows per g
+    const int ng = a.rows / a.bl;
+    dim3 grid(a.bl, ng);
+    fft_large_kernel<MODE, LGM><<<grid, M / 16, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+template <int LGM>
+static int launch_large(const CztArgs &a, cudaStream_t s)
+{
+    switch (a.mode) {
+    case CZT_ANA_BETA: return launch_large_t<CZT_ANA_BETA, LGM>(a, s);
+    case CZT_ANA_ALPHA: return launch_large_t<CZT_ANA_ALPHA, LGM>(a, s);
+    case CZT_SYN_ALPHA: return launch_large_t<CZT_SYN_ALPHA, LGM>(a, s);
+    case CZT_SYN_BETA: return launch_large_t<CZT_SYN_BETA, LGM>(a, s);
+    case FFT_ANA_BETA: return launch_large_t<FFT_ANA_BETA, LGM>(a, s);
+    case FFT_SYN_BETA: return launch_large_t<FFT_SYN_BETA, LGM>(a, s);
+    }
+    return set_error(S2DWC_ERROR_ARG_INVALID, "unknown transform mode %d", a.mode);
+}
+
+static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
     const int M = a.czt.M;
     if (M < 16 || M > 8192 || (M & (M - 1)))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "transform size %d unsupported", M);
+    if (a.rows % a.bl == 0 && g_fft_values != 0) {
+        if (M == 4096) return launch_large<12>(a, s);
+        if (M == 8192) return launch_large<13>(a, s);
+    }
     if (g_fft_values == 16) return M <= 4096 ? launch_fft_mode<16, 256>(a, s) : launch_fft_mode<16, 512>(a, s);
     return M <= 4096 ? launch_fft_mode<8, 512>(a, s) : launch_fft_mode<8, 1024>(a, s);
 }
 
-void set_fft_values(int v) { g_fft_values = (v == 16) ? 16 : 8; }
+void set_fft_values(int v) { g_fft_values = (v == 16) ? 16 : (v == 0 ? 0 : 8); }
 
 int launch_combine(const CombineArgs &a, cudaStream_t s)
 {
