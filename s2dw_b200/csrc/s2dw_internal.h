@@ -113,6 +113,8 @@ struct LwalkArgs {
     int Gs;               // roundup(bl, 32)
     const double2 *F;     // [l*Bp + m] = Om(l,m) flm(l,m)
     double2 *Tg;          // [g][m][m'] N x bl x bl
+    const int2 *tiles;    // (p-tile, m-tile) per CTA, longest walks first
+    int ntiles;
 };
 
 struct MwalkArgs {
@@ -126,7 +128,15 @@ struct MwalkArgs {
     const double2 *V2f;   // [(q*bl + m)*Vs + m']
     int Vs;               // roundup(bl, 8)
     double2 *part;        // this scale's flm contribution [(l-blo-1)*bl + m], m <= l
+    const int2 *tiles;    // (l-tile, m-tile) per CTA, longest walks first
+    int ntiles;
 };
+// Tile lists of the contraction kernels for one scale, ordered by decreasing
+// work so that the longest walks start first.
+void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t);
+void build_mwalk_tiles(int bl, int blo, int wq, std::vector<int2> &t);
+int lwalk_tile_m(int NP);  // m values per lwalk CTA tile
+int mwalk_tile_m(int NP);  // m values per mwalk CTA tile
 
 // flm(l,m) = sum_j part_j(l,m) + Phi2(l) scoeff(l,m), the scale sum of
 // s2dw_core_mod.f90:1228-1253 in scale order followed by :1258-1261.
@@ -169,7 +179,8 @@ int launch_gprep(const GprepArgs &a, cudaStream_t s);
 int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp, cudaStream_t s);
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
-void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread
+void set_fft_values(int v);
+void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels  // FFT engine variant: 8 or 16 values per thread
 int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
 int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,

@@ -13,7 +13,9 @@
 //                    the FFTW alpha transforms (:746-768, :1104-1130).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
+#include <vector>
 #include <cstdio>
 #include <type_traits>
 
@@ -101,7 +103,7 @@ struct LwalkSmem {
 };
 
 template <int NP, int S>
-__global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles_p)
+__device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
 {
     using L = LwalkSmem<NP, S>;
     constexpr int WS = L::WS;
@@ -109,8 +111,8 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
     double2 *sPh = reinterpret_cast<double2 *>(lsm + 2 * L::BUF);  // [g*16 + n+N-1]
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int pt = blockIdx.x % tiles_p, mt = blockIdx.x / tiles_p;
-    const int p0 = pt * 32, m0 = mt * WS;
+    const int2 tile = a.tiles[blockIdx.x];
+    const int p0 = tile.x * 32, m0 = tile.y * WS;
     const int B = a.B, Bp = a.Bp, bl = a.bl, blo = a.blo, N = a.N, Gs = a.Gs;
     const int mp = p0 + lane;
 
@@ -304,6 +306,18 @@ __global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a, int tiles
     }
 }
 
+// MINB = 0: no minimum-blocks bound (the compiler picks the register count)
+template <int NP, int S, int MINB>
+__global__ void __launch_bounds__(LW_W * 32) lwalk_kernel(LwalkArgs a)
+{
+    lwalk_body<NP, S>(a);
+}
+template <int NP, int S, int MINB>
+__global__ void __launch_bounds__(LW_W * 32, MINB) lwalk_kernel_minb(LwalkArgs a)
+{
+    lwalk_body<NP, S>(a);
+}
+
 // Per-scale factor tables for the contraction kernels (built once per set of
 // kernel tables).
 __global__ void gprep_kernel(GprepArgs a)
@@ -368,14 +382,15 @@ struct MwalkSmem {
 };
 
 template <int NP, int Q>
-__global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles_m)
+__device__ __forceinline__ void mwalk_body(const MwalkArgs &a)
 {
     using L = MwalkSmem<NP, Q>;
     constexpr int WQ = L::WQ;
     extern __shared__ __align__(16) double msm[];
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int mt = blockIdx.x % tiles_m, lt = blockIdx.x / tiles_m;
+    const int2 tile = a.tiles[blockIdx.x];
+    const int lt = tile.x, mt = tile.y;
     const int B = a.B, Bp = a.Bp, bl = a.bl, blo = a.blo, Gs = a.Gs, Vs = a.Vs;
     const int lbase = blo + 1 + lt * 32, mbase = mt * WQ;
     const int MH = min(lbase + 31, bl - 1);
@@ -515,6 +530,17 @@ __global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a, int tiles
         const int m = mbase + w * Q + q;
         a.part[(size_t)(l - blo - 1) * bl + m] = cipow(cscale(acc[q], sc), m);
     }
+}
+
+template <int NP, int Q, int MINB>
+__global__ void __launch_bounds__(MW_W * 32) mwalk_kernel(MwalkArgs a)
+{
+    mwalk_body<NP, Q>(a);
+}
+template <int NP, int Q, int MINB>
+__global__ void __launch_bounds__(MW_W * 32, MINB) mwalk_kernel_minb(MwalkArgs a)
+{
+    mwalk_body<NP, Q>(a);
 }
 
 // ===========================================================================
@@ -1185,7 +1211,7 @@ __global__ void combine_kernel(CombineArgs a)
 // ===========================================================================
 // Launchers
 // ===========================================================================
-template <int NP, int S>
+template <int NP, int S, int MINB>
 static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 {
     using L = LwalkSmem<NP, S>;
@@ -1193,28 +1219,82 @@ static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        S2DW_CUDA_TRY(cudaFuncSetAttribute(lwalk_kernel<NP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)L::BYTES));
+        if (MINB > 0)
+            S2DW_CUDA_TRY(cudaFuncSetAttribute(lwalk_kernel_minb<NP, S, (MINB > 0 ? MINB : 1)>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
+        else
+            S2DW_CUDA_TRY(cudaFuncSetAttribute(lwalk_kernel<NP, S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)L::BYTES));
         attr[dev] = true;
     }
-    const int tiles_p = (a.bl + 31) / 32, tiles_m = (a.bl + L::WS - 1) / L::WS;
-    lwalk_kernel<NP, S><<<tiles_p * tiles_m, LW_W * 32, L::BYTES, s>>>(a, tiles_p);
+    if (a.ntiles <= 0) return S2DWC_OK;
+    if (MINB > 0)
+        lwalk_kernel_minb<NP, S, (MINB > 0 ? MINB : 1)><<<a.ntiles, LW_W * 32, L::BYTES, s>>>(a);
+    else
+        lwalk_kernel<NP, S, 0><<<a.ntiles, LW_W * 32, L::BYTES, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
 
-int launch_lwalk(const LwalkArgs &a, cudaStream_t s)
+static int g_lwalk_variant = 0, g_mwalk_variant = 0;
+
+int lwalk_tile_m(int) { return LW_W * (g_lwalk_variant == 1 ? 4 : 4); }
+int mwalk_tile_m(int) { return MW_W * (g_mwalk_variant == 1 ? 8 : 4); }
+
+void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t)
+{
+    // work of tile (pt, mt): walk from max(p0, m0) to bl-1
+    t.clear();
+    const int tp = (bl + 31) / 32, tm = (bl + ws - 1) / ws;
+    for (int pt = 0; pt < tp; pt++)
+        for (int mt = 0; mt < tm; mt++) t.push_back(make_int2(pt, mt));
+    std::stable_sort(t.begin(), t.end(), [ws](int2 a, int2 b) {
+        return std::max(a.x * 32, a.y * ws) < std::max(b.x * 32, b.y * ws);
+    });
+    (void)blo;
+}
+
+void build_mwalk_tiles(int bl, int blo, int wq, std::vector<int2> &t)
+{
+    // tile (lt, mt) covers l in [blo+1+32 lt, +32), m in [wq mt, +wq); its
+    // walk length is ~ the largest l; tiles entirely above m <= l are dropped
+    t.clear();
+    const int nl = bl - blo - 1;
+    if (nl <= 0) return;
+    const int tl = (nl + 31) / 32, tm = (bl + wq - 1) / wq;
+    for (int lt = tl - 1; lt >= 0; lt--) {
+        const int lmax = std::min(blo + 1 + lt * 32 + 31, bl - 1);
+        for (int mt = 0; mt < tm; mt++)
+            if (mt * wq <= lmax) t.push_back(make_int2(lt, mt));
+    }
+}
+void set_walk_variants(int lw, int mw)
+{
+    g_lwalk_variant = lw;
+    g_mwalk_variant = mw;
+}
+
+template <int S, int MINB>
+static int launch_lwalk_s(const LwalkArgs &a, cudaStream_t s)
 {
     switch (a.NP) {
-    case 1: return launch_lwalk_np<1, 4>(a, s);
-    case 2: return launch_lwalk_np<2, 4>(a, s);
-    case 3: return launch_lwalk_np<3, 4>(a, s);
-    case 4: return launch_lwalk_np<4, 4>(a, s);
+    case 1: return launch_lwalk_np<1, S, MINB>(a, s);
+    case 2: return launch_lwalk_np<2, S, MINB>(a, s);
+    case 3: return launch_lwalk_np<3, S, MINB>(a, s);
+    case 4: return launch_lwalk_np<4, S, MINB>(a, s);
     }
     return set_error(S2DWC_ERROR_SIZE_INVALID, "lwalk: unsupported N=%d (N<=8)", a.N);
 }
 
-template <int NP, int Q>
+int launch_lwalk(const LwalkArgs &a, cudaStream_t s)
+{
+    switch (g_lwalk_variant) {
+    case 1: return launch_lwalk_s<4, 4>(a, s);
+    default: return launch_lwalk_s<4, 0>(a, s);
+    }
+}
+
+template <int NP, int Q, int MINB>
 static int launch_mwalk_np(const MwalkArgs &a, cudaStream_t s)
 {
     using L = MwalkSmem<NP, Q>;
@@ -1224,25 +1304,41 @@ static int launch_mwalk_np(const MwalkArgs &a, cudaStream_t s)
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        S2DW_CUDA_TRY(cudaFuncSetAttribute(mwalk_kernel<NP, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)L::BYTES));
+        if (MINB > 0)
+            S2DW_CUDA_TRY(cudaFuncSetAttribute(mwalk_kernel_minb<NP, Q, (MINB > 0 ? MINB : 1)>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
+        else
+            S2DW_CUDA_TRY(cudaFuncSetAttribute(mwalk_kernel<NP, Q, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)L::BYTES));
         attr[dev] = true;
     }
-    const int tiles_l = (nl + 31) / 32, tiles_m = (a.bl + L::WQ - 1) / L::WQ;
-    mwalk_kernel<NP, Q><<<tiles_l * tiles_m, MW_W * 32, L::BYTES, s>>>(a, tiles_m);
+    if (a.ntiles <= 0) return S2DWC_OK;
+    if (MINB > 0)
+        mwalk_kernel_minb<NP, Q, (MINB > 0 ? MINB : 1)><<<a.ntiles, MW_W * 32, L::BYTES, s>>>(a);
+    else
+        mwalk_kernel<NP, Q, 0><<<a.ntiles, MW_W * 32, L::BYTES, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
 
-int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
+template <int Q, int MINB>
+static int launch_mwalk_q(const MwalkArgs &a, cudaStream_t s)
 {
     switch (a.NP) {
-    case 1: return launch_mwalk_np<1, 8>(a, s);
-    case 2: return launch_mwalk_np<2, 8>(a, s);
-    case 3: return launch_mwalk_np<3, 8>(a, s);
-    case 4: return launch_mwalk_np<4, 8>(a, s);
+    case 1: return launch_mwalk_np<1, Q, MINB>(a, s);
+    case 2: return launch_mwalk_np<2, Q, MINB>(a, s);
+    case 3: return launch_mwalk_np<3, Q, MINB>(a, s);
+    case 4: return launch_mwalk_np<4, Q, MINB>(a, s);
     }
     return set_error(S2DWC_ERROR_SIZE_INVALID, "mwalk: unsupported N=%d (N<=8)", a.N);
+}
+
+int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
+{
+    switch (g_mwalk_variant) {
+    case 1: return launch_mwalk_q<8, 0>(a, s);
+    default: return launch_mwalk_q<4, 4>(a, s);
+    }
 }
 
 int launch_gprep(const GprepArgs &a, cudaStream_t s)

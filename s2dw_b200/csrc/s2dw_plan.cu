@@ -52,6 +52,8 @@ struct s2dwc_plan {
     double2 *wsA = nullptr, *wsC = nullptr, *wsP = nullptr;
     std::vector<long long> offA, offC, offP;
     std::vector<cudaStream_t> streams;
+    std::vector<int2 *> lw_tiles, mw_tiles;   // per-scale tile lists (device)
+    std::vector<int> lw_ntiles, mw_ntiles;
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> ev_join;
     // device buffers of the host-buffer entry points (allocated on first use)
@@ -246,6 +248,20 @@ int plan_build(s2dwc_plan *p)
     if ((st = dev_alloc(p, &p->wsA, (size_t)nA)) || (st = dev_alloc(p, &p->wsC, (size_t)nC)) ||
         (st = dev_alloc(p, &p->wsP, (size_t)std::max(1LL, nP))))
         return st;
+    for (int j = 0; j <= J; j++) {
+        std::vector<int2> tl;
+        build_lwalk_tiles(p->bl[j], p->blo[j], lwalk_tile_m(p->NP), tl);
+        int2 *d = nullptr;
+        if ((st = dev_upload(p, &d, tl))) return st;
+        p->lw_tiles.push_back(d);
+        p->lw_ntiles.push_back((int)tl.size());
+        build_mwalk_tiles(p->bl[j], p->blo[j], mwalk_tile_m(p->NP), tl);
+        d = nullptr;
+        if (tl.empty()) tl.push_back(make_int2(0, 0));  // keep a valid allocation
+        if ((st = dev_upload(p, &d, tl))) return st;
+        p->mw_tiles.push_back(d);
+        p->mw_ntiles.push_back(p->bl[j] - p->blo[j] - 1 > 0 ? (int)tl.size() : 0);
+    }
     p->streams.resize(J + 1);
     p->ev_join.resize(J + 1);
     for (int j = 0; j <= J; j++) {
@@ -360,6 +376,8 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         la.Gs = p->ga_stride[j];
         la.F = p->Fw;
         la.Tg = Tg;
+        la.tiles = p->lw_tiles[j];
+        la.ntiles = p->lw_ntiles[j];
         {
             KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
             if ((st = launch_lwalk(la, sj))) return st;
@@ -456,6 +474,8 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ma.V2f = V2f;
         ma.Vs = p->gs_stride[j];
         ma.part = p->wsP + p->offP[j];
+        ma.tiles = p->mw_tiles[j];
+        ma.ntiles = p->mw_ntiles[j];
         {
             KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
             if ((st = launch_mwalk(ma, sj))) return st;
@@ -537,6 +557,10 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         return set_error(S2DWC_ERROR_ARG_INVALID, "device %d out of range (%d devices)", device, ndev);
     DeviceGuard dg(device);
     if (const char *fv = getenv("S2DW_FFT_VALUES")) set_fft_values(atoi(fv));
+    {
+        const char *lw = getenv("S2DW_LWALK_VARIANT"), *mw = getenv("S2DW_MWALK_VARIANT");
+        set_walk_variants(lw ? atoi(lw) : 0, mw ? atoi(mw) : 0);
+    }
     auto *p = new s2dwc_plan();
     p->B = B;
     p->N = N;
