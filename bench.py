@@ -36,7 +36,7 @@ UNIT = "pairs/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--B", type=int, default=1024)
@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--alpha", type=float, default=2.0)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=4096,
+                    help="mixed request stream for the serving p50/p99 (0 = skip)")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of replaying a CUDA graph")
     return ap.parse_args()
 
 
@@ -121,6 +124,44 @@ def contraction_flops_per_scale(B, N, alpha, J):
         ana.append(fa)
         syn.append(fs)
     return ana, syn
+
+
+def serving_stats(n_requests, device):
+    """configs[3]-style stream: Poisson arrivals, B uniform over
+    {32,...,1024}, N uniform over 1..8, alpha in {2,3}, J=Jmax, half analyses
+    and half syntheses (inputs from analyses of seeded maps).  The arrival
+    rate is 70% of the throughput measured with every request arriving at
+    once, so that queues stay finite and the percentiles reflect overlap."""
+    from s2dw_b200.serving import Server, make_stream
+
+    reqs, inputs = make_stream(n_requests, seed=2026, rate_hz=1e9)
+    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device)
+    # warm the plan/graph cache with one request per (config, kind)
+    seen, warm = set(), []
+    for r in reqs:
+        k = (r.B, r.N, r.alpha, r.J, r.kind)
+        if k not in seen:
+            seen.add(k)
+            warm.append(r)
+    for r in warm:
+        r.arrival = 0.0
+    srv.run(warm)
+    for r in reqs:
+        r.arrival = 0.0
+    cap = srv.run(reqs)["throughput_rps"]
+    rate = 0.7 * cap
+    rng = np.random.default_rng(7)
+    t = 0.0
+    for r in reqs:
+        t += rng.exponential(1.0 / rate)
+        r.arrival = t
+    st = srv.run(reqs)
+    srv.close()
+    del inputs
+    st.update({"offered_rate_rps": rate, "saturation_rps": cap, "form": "fp64",
+               "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
+                         "half analysis / half synthesis, device-resident inputs, graph replay"})
+    return st
 
 
 def fft_flops_per_pair(B, N, alpha, J):
@@ -260,9 +301,27 @@ def main():
     d_out = torch.empty_like(d_flm[0])
     stream = torch.cuda.current_stream()
 
-    def step(i):
+    def direct_step(i):
         plan.analysis(d_flm[i % nring], d_wav, d_sc, stream)
         plan.synthesis(d_wav, d_sc, d_out, stream)
+
+    graphs = []
+    if not args.no_graph:
+        direct_step(0)  # kernel attributes are set outside capture
+        torch.cuda.synchronize()
+        cap_stream = torch.cuda.Stream()  # capture needs a non-default stream
+        for i in range(nring):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=cap_stream):
+                plan.analysis(d_flm[i], d_wav, d_sc, torch.cuda.current_stream())
+                plan.synthesis(d_wav, d_sc, d_out, torch.cuda.current_stream())
+            graphs.append(g)
+
+    def step(i):
+        if graphs:
+            graphs[i % nring].replay()
+        else:
+            direct_step(i)
 
     for i in range(args.warmup):
         step(i)
@@ -294,7 +353,7 @@ def main():
     plan.set_timing(True)
     plan.timing(reset=True)
     for i in range(ksteps):
-        step(i)
+        direct_step(i)
     torch.cuda.synchronize()
     kt = plan.timing(reset=True)
     plan.set_timing(False)
@@ -366,6 +425,14 @@ def main():
                "recon_err": e2e_recon,
                "api": "s2dwc_analysis_flm2wav_dynamic + s2dwc_synthesis_wav2flm_dynamic, pinned host buffers"}
 
+    graphs.clear()
+    serving = None
+    if args.serving_requests > 0:
+        try:
+            serving = serving_stats(args.serving_requests, local)
+        except Exception as ex:
+            serving = {"error": str(ex)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -382,9 +449,10 @@ def main():
             "config": {"workload": f"B={B} N={N} alpha={alpha:g} J=Jmax={J} analysis+synthesis of one map per step",
                        "B": B, "N": N, "alpha": alpha, "J": J, "form": "fp64 plain",
                        "parallelism": f"replicas x{world} (no collective)",
+                       "launch": "direct" if args.no_graph else "CUDA graph replay of the pair",
                        "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
                        "recon_err": recon},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
             "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
         }
         print(json.dumps(line), flush=True)

@@ -123,8 +123,22 @@ int plan_build(s2dwc_plan *p)
         band_limits(j, B, p->alpha, &p->bl[j], &p->blo[j]);
         p->wav_off[j + 1] = p->wav_off[j] + (long long)(2 * p->bl[j] - 1) * (2 * p->bl[j]) * N;
     }
-    RecTables t;
-    build_rec_tables(B, t);
+    // host tables depend only on B: build once per process
+    static std::mutex rec_mu;
+    static std::map<int, std::shared_ptr<RecTables>> rec_cache;
+    std::shared_ptr<RecTables> tp;
+    {
+        std::lock_guard<std::mutex> g(rec_mu);
+        auto it = rec_cache.find(B);
+        if (it == rec_cache.end()) {
+            tp = std::make_shared<RecTables>();
+            build_rec_tables(B, *tp);
+            rec_cache[B] = tp;
+        } else {
+            tp = it->second;
+        }
+    }
+    const RecTables &t = *tp;
     // row-padded copies (stride Bp) of the tables read by 32-wide tiles
     const int Bp = (B + 31) / 32 * 32;
     p->Bp = Bp;

@@ -1,0 +1,289 @@
+"""Continuous-batching server for mixed S2DW transform requests on one GPU.
+
+Requests are analyses (flm -> wav) or syntheses (wav -> flm) of any supported
+(B, N, alpha, J).  A request is admitted as soon as a *slot* for its
+configuration is free: a slot is a plan (cached recurrence and chirp tables,
+workspaces, per-scale streams) with its own output buffers and CUDA stream.
+Slots are created on demand while the device memory they hold stays within
+an HBM budget; when the budget is full an idle slot of another configuration
+is evicted (least recently used) or the request waits.  Admitted requests run
+concurrently on their slots' streams, so work of requests that arrive while
+others are on the GPU overlaps on the device.  Each slot replays a CUDA graph
+captured once per (kind, input buffer), which removes the per-kernel launch
+cost of the ~20-70 kernels a transform issues.
+
+Results are identical alone and in a mix: the kernels are deterministic (no
+atomics; the synthesis sums scales in a fixed order), and a slot's buffers are
+owned by one request at a time.
+
+Latency of a request = device time of its completion event minus its arrival
+time, both relative to the stream's start (an event recorded when the first
+request is admitted).
+"""
+import collections
+import dataclasses
+import time
+
+import numpy as np
+
+from .device import Plan
+from .workload import transform_setup
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    kind: str                 # "analysis" or "synthesis"
+    B: int
+    N: int
+    alpha: float
+    J: int
+    arrival: float            # seconds after the stream start
+    inp: tuple = ()           # device tensors: (flm,) or (wav, scoeff)
+    # filled by the server
+    slot_key: tuple = None
+    done_event: object = None
+    t_done: float = None      # seconds after the stream start (device clock)
+    out: object = None        # host copy of the output when keep_outputs
+
+
+class Slot:
+    def __init__(self, key, tables, device):
+        import torch
+
+        B, N, alpha, J = key
+        self.key = key
+        self.plan = Plan(B, N, alpha, J, device=device)
+        self.plan.set_tables(tables["K_gamma"], tables["Phi2"], tables["Slm"], tables["bl_scoeff"])
+        bs = tables["bl_scoeff"]
+        self.stream = torch.cuda.Stream(device=device)
+        self.d_wav = torch.empty(self.plan.wav_size, dtype=torch.float64, device=device)
+        self.d_sc = torch.empty(max(1, bs * bs), dtype=torch.complex128, device=device)
+        self.d_flm = torch.empty((B, B), dtype=torch.complex128, device=device)
+        self.bytes = self.plan.workspace_bytes() + 8 * self.plan.wav_size + 16 * (bs * bs + B * B)
+        self.graphs = {}
+        self.busy = False
+        self.last_used = 0.0
+
+    def run(self, req, use_graphs):
+        """Enqueue the request's transform on this slot's stream."""
+        import torch
+
+        def body():
+            if req.kind == "analysis":
+                self.plan.analysis(req.inp[0], self.d_wav, self.d_sc, stream=torch.cuda.current_stream())
+            else:
+                self.plan.synthesis(req.inp[0], req.inp[1], self.d_flm, stream=torch.cuda.current_stream())
+
+        with torch.cuda.stream(self.stream):
+            if use_graphs:
+                gkey = (req.kind,) + tuple(t.data_ptr() for t in req.inp)
+                g = self.graphs.get(gkey)
+                if g is None:
+                    body()  # warm-up launch outside capture (lazy kernel attributes)
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=self.stream):
+                        body()
+                    self.graphs[gkey] = g
+                g.replay()
+            else:
+                body()
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(self.stream)
+        return ev
+
+    def output(self, req):
+        return (self.d_wav, self.d_sc) if req.kind == "analysis" else (self.d_flm,)
+
+    def close(self):
+        self.graphs.clear()
+        self.plan.close()
+
+
+class Server:
+    def __init__(self, hbm_budget_bytes=40 << 30, max_inflight=64, slots_per_config=2, use_graphs=True,
+                 device=0, keep_outputs=False):
+        self.budget = int(hbm_budget_bytes)
+        self.max_inflight = max_inflight
+        self.slots_per_config = slots_per_config
+        self.use_graphs = use_graphs
+        self.device = device
+        self.keep_outputs = keep_outputs
+        self.slots = collections.defaultdict(list)  # key -> [Slot]
+        self.tables = {}
+        self.used = 0
+
+    def config_tables(self, B, N, alpha, J):
+        key = (B, N, alpha, J)
+        if key not in self.tables:
+            self.tables[key] = transform_setup(B, N, alpha, J)
+        return self.tables[key]
+
+    def _evict_one(self, keep_key):
+        idle = [s for k, lst in self.slots.items() if k != keep_key for s in lst if not s.busy]
+        if not idle:
+            return False
+        victim = min(idle, key=lambda s: s.last_used)
+        self.slots[victim.key].remove(victim)
+        self.used -= victim.bytes
+        victim.close()
+        return True
+
+    def _acquire(self, key, now):
+        for s in self.slots[key]:
+            if not s.busy:
+                return s
+        if len(self.slots[key]) >= self.slots_per_config:
+            return None
+        B, N, alpha, J = key
+        # size estimate of a new slot; evict idle slots of other configs if needed
+        est = Slot.estimate_bytes(B, N, alpha, J)
+        while self.used + est > self.budget:
+            if not self._evict_one(key):
+                return None
+        s = Slot(key, self.config_tables(B, N, alpha, J), self.device)
+        self.slots[key].append(s)
+        self.used += s.bytes
+        return s
+
+    def run(self, requests, poll_sleep=0.0):
+        """Serves `requests` (sorted by arrival) with wall-clock arrivals.
+        Returns a dict of latency/throughput statistics."""
+        import torch
+
+        torch.cuda.set_device(self.device)
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        waiting = collections.deque()
+        inflight = []
+        done = []
+        base = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        base.record()
+        while pending or waiting or inflight:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            # admit in arrival order; a request whose config has no free slot
+            # does not block requests of other configs
+            still = collections.deque()
+            while waiting:
+                r = waiting.popleft()
+                if len(inflight) >= self.max_inflight:
+                    still.append(r)
+                    continue
+                key = (r.B, r.N, r.alpha, r.J)
+                s = self._acquire(key, now)
+                if s is None:
+                    still.append(r)
+                    continue
+                s.busy = True
+                s.last_used = now
+                r.slot_key = key
+                r.done_event = s.run(r, self.use_graphs)
+                inflight.append((r, s))
+            waiting = still
+            rest = []
+            for r, s in inflight:
+                if r.done_event.query():
+                    r.t_done = base.elapsed_time(r.done_event) / 1e3
+                    if self.keep_outputs:
+                        r.out = tuple(t.detach().cpu().numpy().copy() for t in s.output(r))
+                    s.busy = False
+                    done.append(r)
+                else:
+                    rest.append((r, s))
+            inflight = rest
+            if not inflight and not waiting and pending:
+                delay = pending[0].arrival - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            elif poll_sleep:
+                time.sleep(poll_sleep)
+        torch.cuda.synchronize()
+        t_end = time.perf_counter() - t0
+        lat = np.array([r.t_done - r.arrival for r in done]) * 1e3
+        span = max(r.t_done for r in done) - min(r.arrival for r in done)
+        return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "throughput_rps": len(done) / span, "wall_s": t_end,
+                "slots": sum(len(v) for v in self.slots.values()), "hbm_bytes": self.used}
+
+    def close(self):
+        for lst in self.slots.values():
+            for s in lst:
+                s.close()
+        self.slots.clear()
+        self.used = 0
+
+
+def _estimate_bytes(B, N, alpha, J):
+    """Device bytes a slot of (B, N, alpha, J) holds (plan + buffers)."""
+    from .core import band_limits
+
+    wav = 0
+    tg = ta = 0
+    for j in range(J + 1):
+        bl, _ = band_limits(j, B, alpha)
+        wav += (2 * bl - 1) * 2 * bl * N
+        tg += N * bl * bl
+        ta += N * bl * 2 * bl
+    Bp = (B + 31) // 32 * 32
+    tables = B * Bp * 8 * 6 + B * B * 8 * 8 + B * B * 16
+    return 8 * wav + 16 * (tg + ta) * 3 // 2 + tables + 16 * B * B * 3
+
+
+Slot.estimate_bytes = staticmethod(_estimate_bytes)
+
+
+def make_stream(n_requests, seed=0, rate_hz=2000.0, Bs=(32, 64, 128, 256, 512, 1024), Ns=range(1, 9),
+                alphas=(2.0, 3.0), device="cuda", pool=2):
+    """The benchmark's mixed request stream: Poisson arrivals at `rate_hz`,
+    B uniform over `Bs`, N uniform over `Ns`, alpha over `alphas`, J = Jmax,
+    half analyses and half syntheses.  Inputs are device-resident: `pool`
+    seeded maps per configuration (analysis inputs from the Gaussian
+    generator; synthesis inputs from an analysis of such a map), shared by the
+    requests of that configuration.  Returns (requests, inputs) where inputs
+    maps config -> list of (flm, wav, scoeff) device tensors."""
+    import torch
+
+    from . import core
+    from .workload import gaussian_flm
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    inputs = {}
+    for i in range(n_requests):
+        t += rng.exponential(1.0 / rate_hz)
+        B = int(rng.choice(Bs))
+        N = int(rng.choice(list(Ns)))
+        alpha = float(rng.choice(alphas))
+        J = core.s2dw_core_comp_Jmax(B, alpha)
+        kind = "analysis" if rng.random() < 0.5 else "synthesis"
+        key = (B, N, alpha, J)
+        if key not in inputs:
+            inputs[key] = None
+        reqs.append(Request(rid=i, kind=kind, B=B, N=N, alpha=alpha, J=J, arrival=t,
+                            inp=(int(rng.integers(pool)),)))
+    # device-resident inputs per configuration
+    for key in inputs:
+        B, N, alpha, J = key
+        tab = transform_setup(B, N, alpha, J)
+        plan = Plan(B, N, alpha, J)
+        plan.set_tables(tab["K_gamma"], tab["Phi2"], tab["Slm"], tab["bl_scoeff"])
+        lst = []
+        for k in range(pool):
+            flm = gaussian_flm(B, seed=1000 * k + B + 17 * N)
+            d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).to(device)
+            d_wav = torch.empty(plan.wav_size, dtype=torch.float64, device=device)
+            d_sc = torch.empty(max(1, tab["bl_scoeff"] ** 2), dtype=torch.complex128, device=device)
+            plan.analysis(d_flm, d_wav, d_sc)
+            lst.append((d_flm, d_wav, d_sc, flm))
+        torch.cuda.synchronize()
+        plan.close()
+        inputs[key] = lst
+    for r in reqs:
+        d_flm, d_wav, d_sc, _ = inputs[(r.B, r.N, r.alpha, r.J)][r.inp[0]]
+        r.inp = (d_flm,) if r.kind == "analysis" else (d_wav, d_sc)
+    return reqs, inputs
