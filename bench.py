@@ -32,6 +32,14 @@ sys.path.insert(0, ROOT)
 METRIC = "B=1024 N=4 analysis+synthesis pairs/s at recon err<=1e-10"
 UNIT = "pairs/s"
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
+# kernel kind, averaged over the 66 launches of each kind in two
+# analysis+synthesis pairs at B=1024 N=4 alpha=2 J=10, from one ncu capture of
+# this script (command and per-kernel table: profiles/traffic_B1024_N4.md).
+# Used only for the roofline "traffic" entry of that workload.
+NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.43e6, "mwalk": 10.77e6, "ana_beta": 27.73e6,
+                                "ana_alpha": 45.15e6, "syn_alpha": 43.53e6, "syn_beta": 56.48e6}}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -370,8 +378,10 @@ def main():
         per_launch_ms = ms / n_launch
         launches_per_pair = n_launch / ksteps
         achieved = algo[dom[0]] / launches_per_pair / (per_launch_ms / 1e3) / 1e12
+        traffic = NCU_TRAFFIC.get((B, N, float(alpha)), {}).get(dom[0])
         roofline = {"kernel": dom[0], "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
-                    "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
+                    "traffic_unit": "bytes per launch (ncu, mean over a pair's launches)",
                     "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (MEASURED_PEAKS.json has no fp64 entry)",
                     "flops_per_pair": algo[dom[0]], "launches_per_pair": launches_per_pair,
                     "avg_launch_ms": per_launch_ms}
