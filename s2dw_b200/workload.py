@@ -43,3 +43,37 @@ def transform_setup(B, N, alpha=2.0, J=None):
     K, P, bs = core.s2dw_core_init_kernels(J, B, alpha)
     S = core.s2dw_core_init_directionality(B, N)
     return {"B": B, "N": N, "alpha": alpha, "J": J, "K_gamma": K, "Phi2": P, "bl_scoeff": bs, "Slm": S}
+
+
+def run_pairs(B, N, alpha=2.0, pairs=2, seed=0):
+    """Runs `pairs` device analysis+synthesis pairs of one seeded map through a
+    plan on cuda:0 and returns the reconstruction error max|f' - f|.  This is
+    the small fixed workload that kernel profiles are captured on:
+    python -m s2dw_b200.workload B N pairs."""
+    import torch
+
+    from .device import Plan
+
+    t = transform_setup(B, N, alpha)
+    plan = Plan(B, N, alpha, t["J"])
+    plan.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    flm = gaussian_flm(B, seed=seed)
+    d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
+    d_wav = torch.empty(plan.wav_size, dtype=torch.float64, device="cuda")
+    d_sc = torch.empty(max(1, t["bl_scoeff"] ** 2), dtype=torch.complex128, device="cuda")
+    d_out = torch.empty_like(d_flm)
+    for _ in range(pairs):
+        plan.analysis(d_flm, d_wav, d_sc)
+        plan.synthesis(d_wav, d_sc, d_out)
+    torch.cuda.synchronize()
+    err = float(np.abs(d_out.cpu().numpy().T - flm).max())
+    plan.close()
+    return err
+
+
+if __name__ == "__main__":
+    import sys
+
+    a = [int(x) for x in sys.argv[1:4]] + [None] * 3
+    B, N, P = a[0] or 1024, a[1] or 4, a[2] or 2
+    print(f"B={B} N={N} pairs={P} recon {run_pairs(B, N, 2.0, P):.3e}")
