@@ -172,6 +172,32 @@ int s2dwc_plan_analysis(s2dwc_plan *plan, double *d_wav, double *d_scoeff, const
 int s2dwc_plan_synthesis(s2dwc_plan *plan, double *d_flm, const double *d_wav,
                          const double *d_scoeff, void *stream);
 
+/* Analysis on device memory that allocates nothing.  This entry point has no
+ * counterpart in the reference.  It computes what s2dwc_plan_analysis
+ * computes, with the same arguments, but takes its workspace (the F table and
+ * one scale's Tg and Tb) from a fixed static device array of
+ * S2DWC_NOALLOC_SCRATCH_BYTES instead of the plan's workspaces, and runs the
+ * scales one after another on `stream`.  It makes no cudaMalloc, cudaFree or
+ * other allocating call.  It is meant for callers that must not allocate
+ * device memory once they are running: a program whose device memory is
+ * already taken by its own pool allocator, or a loop in which an allocation
+ * would synchronise the device and stall other streams.
+ *  - Limit: the plan must need at most S2DWC_NOALLOC_SCRATCH_BYTES of scratch
+ *    (16 (B B_pad + 3 N B^2) bytes, B_pad = B rounded up to a multiple of
+ *    32, plus alignment): any B <= 256 with N <= 8, or B = 512 with N <= 2.  Larger plans are
+ *    rejected with S2DWC_ERROR_SIZE_INVALID.
+ *  - Setup: the first call on a device looks up the array's address
+ *    (cudaGetSymbolAddress), which makes the CUDA driver load the module that
+ *    holds it; make that first call during setup, before any stream capture.
+ *  - Nothing needs to start at zero: each call writes every scratch element
+ *    before it reads it.
+ *  - There is one scratch array per device: calls that overlap in time on one
+ *    device (different streams or host threads without ordering between them)
+ *    race on it.  Order them on one stream or with events. */
+#define S2DWC_NOALLOC_SCRATCH_BYTES (32LL << 20)
+int s2dwc_plan_analysis_noalloc(const s2dwc_plan *plan, double *d_wav, double *d_scoeff,
+                                const double *d_flm, void *stream);
+
 /* Number of CUDA kernels one analysis / one synthesis launches. */
 int s2dwc_plan_launch_count(const s2dwc_plan *plan, int *analysis, int *synthesis);
 

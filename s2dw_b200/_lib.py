@@ -40,6 +40,7 @@ SIGNATURES = {
     "s2dwc_plan_workspace_bytes": (ctypes.c_longlong, [_vp]),
     "s2dwc_plan_analysis": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_synthesis": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "s2dwc_plan_analysis_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_launch_count": (_i, [_vp, _ip, _ip]),
     "s2dwc_plan_set_timing": (_i, [_vp, _i]),
     "s2dwc_plan_timing": (_i, [_vp, _i, _llp, _dp]),

@@ -187,4 +187,8 @@ int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, 
                        cudaStream_t s);
 int launch_combine(const CombineArgs &a, cudaStream_t s);
 
+// Address on `device` (which must be current) of the static scratch array of
+// s2dwc_plan_analysis_noalloc, looked up once per device.
+int noalloc_scratch(int device, void **ptr);
+
 }  // namespace s2dw

@@ -515,6 +515,81 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
     return launch_combine(cb, s);
 }
 
+// Layout of the caller-independent workspace of run_analysis_serial: the F
+// table, then one scale's Tg and Tb at the largest band limit, each region
+// starting on a 256-byte boundary.
+struct SerialLayout {
+    long long offTg, offTb, bytes;
+};
+
+SerialLayout serial_layout(const s2dwc_plan *p)
+{
+    auto up = [](long long x) { return (x + 255) / 256 * 256; };
+    const long long b = *std::max_element(p->bl.begin(), p->bl.end());
+    SerialLayout L;
+    L.offTg = up((long long)p->B * p->Bp * (long long)sizeof(double2));
+    L.offTb = L.offTg + up((long long)p->N * b * b * (long long)sizeof(double2));
+    L.bytes = L.offTb + (long long)p->N * b * 2 * b * (long long)sizeof(double2);
+    return L;
+}
+
+// The analysis of run_analysis with its F table and per-scale workspaces in
+// `ws` (serial_layout bytes) instead of the plan's: every launch on `s`, the
+// scales one after another, so that each scale reuses the same Tg and Tb.
+// Every element a kernel reads here is written earlier in the same call, so
+// `ws` needs no initial contents.
+int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, double2 *d_scoeff,
+                        const double2 *d_flm, cudaStream_t s)
+{
+    const SerialLayout L = serial_layout(p);
+    double2 *F = reinterpret_cast<double2 *>(ws);
+    double2 *Tg = reinterpret_cast<double2 *>(ws + L.offTg), *Tb = reinterpret_cast<double2 *>(ws + L.offTb);
+    int st;
+    if ((st = launch_fprep(F, d_flm, p->Om, p->B, p->Bp, s))) return st;
+    for (int j = 0; j <= p->J; j++) {
+        const int bl = p->bl[j];
+        LwalkArgs la{};
+        la.B = p->B;
+        la.Bp = p->Bp;
+        la.N = p->N;
+        la.NP = p->NP;
+        la.bl = bl;
+        la.blo = p->blo[j];
+        std::memcpy(la.nq, p->nq, sizeof(la.nq));
+        la.Acoef = p->Acoef;
+        la.Stm = p->Stm;
+        la.Ste = p->Ste;
+        la.G = p->Ga + p->ga_off[j];
+        la.Gs = p->ga_stride[j];
+        la.F = F;
+        la.Tg = Tg;
+        la.tiles = p->lw_tiles[j];
+        la.ntiles = p->lw_ntiles[j];
+        if ((st = launch_lwalk(la, s))) return st;
+        CztArgs ca{};
+        ca.mode = p->ana_beta_mode[j];
+        ca.bl = bl;
+        ca.N = p->N;
+        ca.NP = p->NP;
+        std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
+        ca.rows = p->N * bl;
+        ca.czt = p->czt[j][ca.mode];
+        ca.tw = p->tw.at(ca.czt.M);
+        ca.in_c = Tg;
+        ca.out_c = Tb;
+        if ((st = launch_czt(ca, s))) return st;
+        ca.mode = CZT_ANA_ALPHA;
+        ca.rows = p->N * bl;
+        ca.czt = p->czt[j][CZT_ANA_ALPHA];
+        ca.tw = p->tw.at(ca.czt.M);
+        ca.in_c = Tb;
+        ca.out_c = nullptr;
+        ca.out_r = d_wav + p->wav_off[j];
+        if ((st = launch_czt(ca, s))) return st;
+    }
+    return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
+}
+
 }  // namespace
 
 extern "C" {
@@ -747,6 +822,27 @@ int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, cons
     DeviceGuard dg(p->device);
     return run_synthesis(p, reinterpret_cast<double2 *>(d_flm), d_wav,
                          reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
+}
+
+int s2dwc_plan_analysis_noalloc(const s2dwc_plan *p, double *d_wav, double *d_scoeff, const double *d_flm,
+                                void *stream)
+{
+    if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_noalloc: null pointer");
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis_noalloc: tables not set");
+    const SerialLayout L = serial_layout(p);
+    if (L.bytes > S2DWC_NOALLOC_SCRATCH_BYTES)
+        return set_error(S2DWC_ERROR_SIZE_INVALID,
+                         "plan_analysis_noalloc: B=%d N=%d needs %lld bytes of scratch, more than the "
+                         "%lld-byte static scratch (it holds B<=256 at any N<=8, or B=512 at N<=2); "
+                         "use s2dwc_plan_analysis",
+                         p->B, p->N, L.bytes, (long long)S2DWC_NOALLOC_SCRATCH_BYTES);
+    DeviceGuard dg(p->device);
+    void *ws = nullptr;
+    int st = noalloc_scratch(p->device, &ws);
+    if (st) return st;
+    return run_analysis_serial(p, static_cast<unsigned char *>(ws), d_wav, reinterpret_cast<double2 *>(d_scoeff),
+                               reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -110,6 +110,17 @@ class Plan:
                                         self._ptr(flm, torch.complex128, self.B * self.B),
                                         self._stream(stream)))
 
+    def analysis_noalloc(self, flm, wav, scoeff, stream=None):
+        """The analysis of `analysis` through s2dwc_plan_analysis_noalloc: its
+        workspace is the library's static device scratch, so the call
+        allocates nothing (plans up to the scratch's size only)."""
+        import torch
+
+        check(lib().s2dwc_plan_analysis_noalloc(self._h, self._ptr(wav, torch.float64, self.wav_size),
+                                                self._ptr(scoeff, torch.complex128, self.bl_scoeff ** 2),
+                                                self._ptr(flm, torch.complex128, self.B * self.B),
+                                                self._stream(stream)))
+
     def synthesis(self, wav, scoeff, flm, stream=None):
         import torch
 
