@@ -53,8 +53,17 @@ extern "C" {
  * failure).  The message names the call. */
 #define S2DWC_ERROR_CUDA 15
 
-/* Precision form of the transform. */
+/* Precision form of the transform.  FP64: every stage in FP64, the drop-in
+ * form.  SPLIT: the analysis contraction runs on the tensor cores as exact
+ * int8 products of 48-bit fixed-point digits (six byte digits per operand,
+ * per-row and per-column power-of-two scales, the 28 most significant digit
+ * products summed exactly in int32), combined in FP64; the d^l(pi/2)
+ * recurrence, the kernel tables and the beta/alpha transforms stay FP64, and
+ * synthesis is the FP64 one.  Its analysis error is bounded by 1e-10 of
+ * max|w| per scale; it pays off for batches of maps
+ * (s2dwc_plan_analysis_batch), which share the d-operand. */
 #define S2DWC_FORM_FP64 0
+#define S2DWC_FORM_SPLIT 1
 
 /* ---------------------------------------------------------------------- */
 /* Library state                                                          */
@@ -145,7 +154,7 @@ typedef struct s2dwc_plan s2dwc_plan;
 
 /* Creates a plan for (B, N, alpha, J) on CUDA device `device`: cached
  * recurrence tables, chirp filters and workspaces.  `form` is
- * S2DWC_FORM_FP64. */
+ * S2DWC_FORM_FP64 or S2DWC_FORM_SPLIT. */
 int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int form, int device);
 int s2dwc_plan_destroy(s2dwc_plan *plan);
 
@@ -171,6 +180,23 @@ int s2dwc_plan_analysis(s2dwc_plan *plan, double *d_wav, double *d_scoeff, const
 /* Synthesis on device memory (d_flm is overwritten). */
 int s2dwc_plan_synthesis(s2dwc_plan *plan, double *d_flm, const double *d_wav,
                          const double *d_scoeff, void *stream);
+
+/* Batches of maps with the same (B, N, alpha, J): map k's flm, packed
+ * wavelets and scoeff start at k*B*B complex values, k*offsets[J+1] doubles
+ * and k*bl_scoeff^2 complex values.  With S2DWC_FORM_SPLIT the analysis runs
+ * the tensor-core contraction on groups of up to 32 maps; otherwise (and for
+ * synthesis) the maps run one after another.  Not in the reference, whose
+ * s2dw_wstats loops s2dw_core_analysis_flm2wav_dynamic over maps
+ * (src/prog/s2dw_wstats.f90:181-197). */
+int s2dwc_plan_analysis_batch(s2dwc_plan *plan, int nmaps, double *d_wav, double *d_scoeff,
+                              const double *d_flm, void *stream);
+int s2dwc_plan_synthesis_batch(s2dwc_plan *plan, int nmaps, double *d_flm, const double *d_wav,
+                               const double *d_scoeff, void *stream);
+
+/* Synchronises with the device and reports S2DWC_ERROR_CUDA if a split-form
+ * kernel gave up waiting on its tensor-core pipeline (each wait is bounded
+ * by 2 s); S2DWC_OK otherwise. */
+int s2dwc_plan_check(s2dwc_plan *plan);
 
 /* Analysis on device memory that allocates nothing.  This entry point has no
  * counterpart in the reference.  It computes what s2dwc_plan_analysis

@@ -41,6 +41,9 @@ SIGNATURES = {
     "s2dwc_plan_analysis": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_synthesis": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_analysis_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "s2dwc_plan_analysis_batch": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "s2dwc_plan_synthesis_batch": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "s2dwc_plan_check": (_i, [_vp]),
     "s2dwc_plan_launch_count": (_i, [_vp, _ip, _ip]),
     "s2dwc_plan_set_timing": (_i, [_vp, _i]),
     "s2dwc_plan_timing": (_i, [_vp, _i, _llp, _dp]),

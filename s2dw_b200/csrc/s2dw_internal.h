@@ -187,6 +187,46 @@ int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, 
                        cudaStream_t s);
 int launch_combine(const CombineArgs &a, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Split-precision analysis contraction (tcgen05 int8 digits, batches of maps)
+// ---------------------------------------------------------------------------
+// Start values below 2^S2DW_SCALE_EXP put a warp of l-walk chains in a scaled
+// domain; values above 2^S2DW_RENORM_EXP there are scaled back down.
+#define S2DW_SCALE_EXP (-600)
+#define S2DW_RENORM_EXP 400
+
+struct SplitArgs {
+    int B, Bp, N, NP, bl, blo;
+    int c0, nch, nmaps;        // first 32-row chunk of l stored in fdig, chunks, maps (<= 32)
+    int nq[4];
+    const double *Acoef, *Om;  // [l*Bp + x]
+    const double *Stm;         // [l0*B + k]
+    const int32_t *Ste;
+    const double *G;           // as LwalkArgs::G
+    int Gs;
+    int16_t *dexp;             // [(m*bl + m')*NP + q] exponent of max_l |v|
+    const int32_t *fexp;       // [m*64 + col] exponent of the map column
+    const uint8_t *fdig;       // [(m*nch + chunk)*5 + digit][2048] map digits
+    double2 *Tg;               // [k][g][m][m'] per map
+    const int2 *tiles;         // (m, chain tile)
+    int ntiles;
+    int *err;                  // set to 1 when a wait gave up
+};
+
+struct FdigArgs {
+    int B, bl, blo, c0, nch, nmaps;
+    const double2 *flm;        // nmaps maps of B*B, flm[l + B*m]
+    int32_t *fexp;
+    uint8_t *fdig;
+};
+
+int split_chains(int NP);       // m' per CTA
+int split_maps_per_pass();      // maps per CTA
+long long split_fdig_bytes(int bl, int nch);
+int launch_split_dexp(const SplitArgs &a, cudaStream_t s);
+int launch_split_fdig(const FdigArgs &a, cudaStream_t s);
+int launch_split(const SplitArgs &a, cudaStream_t s);
+
 // Address on `device` (which must be current) of the static scratch array of
 // s2dwc_plan_analysis_noalloc, looked up once per device.
 int noalloc_scratch(int device, void **ptr);

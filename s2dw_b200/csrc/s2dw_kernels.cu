@@ -58,11 +58,6 @@ __device__ __forceinline__ int warp_max_i(int v)
     return v;
 }
 
-// Exponent below which a warp works in a scaled domain: start values below
-// 2^-600 are multiplied by 2^Kw so that the recurrence cannot underflow
-// (B > ~1000 has edge values down to 2^-B).
-#define S2DW_SCALE_EXP (-600)
-#define S2DW_RENORM_EXP 400
 
 // ===========================================================================
 // Asynchronous global -> shared copies (16 bytes, L2 only)

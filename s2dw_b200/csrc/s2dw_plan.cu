@@ -66,6 +66,19 @@ struct s2dwc_plan {
     std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> tev;
     double t_ms[S2DWC_KIND_COUNT] = {0};
     long long t_n[S2DWC_KIND_COUNT] = {0};
+    // split-precision form (S2DWC_FORM_SPLIT): built on first use
+    struct SplitScale {
+        int c0 = 0, nch = 0, ntiles = 0;
+        int2 *tiles = nullptr;
+        long long dexp_off = 0;
+    };
+    std::vector<SplitScale> sp;
+    bool sp_alloc = false, sp_dexp_valid = false;
+    int16_t *sp_dexp = nullptr;
+    int32_t *sp_fexp = nullptr;
+    uint8_t *sp_fdig = nullptr;
+    double2 *sp_Tg = nullptr, *sp_Tb = nullptr;
+    int *sp_err = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
 
@@ -590,6 +603,168 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
     return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
 }
 
+// Split form: workspaces, tile lists and the per-row exponent tables (the
+// latter depend on the kernel tables and are rebuilt after set_tables).
+int split_prepare(s2dwc_plan *p, cudaStream_t s)
+{
+    int st;
+    const int NP = p->NP, CH = split_chains(NP), MAPS = split_maps_per_pass();
+    if (!p->sp_alloc) {
+        p->sp.resize(p->J + 1);
+        long long nd = 0, fdig = 0;
+        int blmax = 0;
+        for (int j = 0; j <= p->J; j++) {
+            auto &S = p->sp[j];
+            const int bl = p->bl[j], blo = p->blo[j];
+            blmax = std::max(blmax, bl);
+            S.c0 = (blo + 1) / 32;
+            S.nch = (bl - 1) / 32 - S.c0 + 1;
+            S.dexp_off = nd;
+            nd += (long long)bl * bl * NP;
+            fdig = std::max(fdig, split_fdig_bytes(bl, S.nch));
+            // (m, chain tile), longest walks (smallest first row) first
+            std::vector<int2> tl;
+            const int np = (bl + CH - 1) / CH;
+            for (int m = 0; m < bl; m++)
+                for (int pt = 0; pt < np; pt++) tl.push_back(make_int2(m, pt));
+            std::stable_sort(tl.begin(), tl.end(), [CH](int2 a, int2 b) {
+                return std::max(a.x, a.y * CH) < std::max(b.x, b.y * CH);
+            });
+            S.ntiles = (int)tl.size();
+            if ((st = dev_upload(p, &S.tiles, tl))) return st;
+        }
+        const long long b2 = (long long)blmax * blmax;
+        if ((st = dev_alloc(p, &p->sp_dexp, (size_t)nd)) || (st = dev_alloc(p, &p->sp_fexp, (size_t)blmax * 64)) ||
+            (st = dev_alloc(p, &p->sp_fdig, (size_t)fdig)) ||
+            (st = dev_alloc(p, &p->sp_Tg, (size_t)MAPS * p->N * b2)) ||
+            (st = dev_alloc(p, &p->sp_Tb, (size_t)p->N * 2 * b2)) || (st = dev_alloc(p, &p->sp_err, 1)))
+            return st;
+        S2DW_CUDA_TRY(cudaMemsetAsync(p->sp_err, 0, sizeof(int), s));
+        p->sp_alloc = true;
+    }
+    if (!p->sp_dexp_valid) {
+        for (int j = 0; j <= p->J; j++) {
+            SplitArgs a{};
+            a.B = p->B;
+            a.Bp = p->Bp;
+            a.N = p->N;
+            a.NP = NP;
+            a.bl = p->bl[j];
+            a.blo = p->blo[j];
+            std::memcpy(a.nq, p->nq, sizeof(a.nq));
+            a.Acoef = p->Acoef;
+            a.Om = p->Om;
+            a.Stm = p->Stm;
+            a.Ste = p->Ste;
+            a.G = p->Ga + p->ga_off[j];
+            a.Gs = p->ga_stride[j];
+            a.dexp = p->sp_dexp + p->sp[j].dexp_off;
+            a.tiles = p->sp[j].tiles;
+            a.ntiles = p->sp[j].ntiles;
+            if ((st = launch_split_dexp(a, s))) return st;
+        }
+        p->sp_dexp_valid = true;
+    }
+    return S2DWC_OK;
+}
+
+// Split-form analysis of `nmaps` maps (flm, wav and scoeff of map k at
+// k * B^2, k * wav_total and k * bl_scoeff^2): per group of up to 32 maps
+// and per scale, the map digits, the tensor-core contraction into Tg of the
+// whole group, then the beta and alpha transforms map by map.
+int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoeff, const double2 *d_flm,
+                       cudaStream_t s)
+{
+    int st;
+    if ((st = split_prepare(p, s))) return st;
+    const int MAPS = split_maps_per_pass();
+    const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
+    const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
+    for (int g0 = 0; g0 < nmaps; g0 += MAPS) {
+        const int nk = std::min(MAPS, nmaps - g0);
+        for (int j = 0; j <= p->J; j++) {
+            const int bl = p->bl[j];
+            const auto &S = p->sp[j];
+            FdigArgs fa{};
+            fa.B = p->B;
+            fa.bl = bl;
+            fa.blo = p->blo[j];
+            fa.c0 = S.c0;
+            fa.nch = S.nch;
+            fa.nmaps = nk;
+            fa.flm = d_flm + g0 * B2;
+            fa.fexp = p->sp_fexp;
+            fa.fdig = p->sp_fdig;
+            {
+                KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+                if ((st = launch_split_fdig(fa, s))) return st;
+            }
+            SplitArgs a{};
+            a.B = p->B;
+            a.Bp = p->Bp;
+            a.N = p->N;
+            a.NP = p->NP;
+            a.bl = bl;
+            a.blo = p->blo[j];
+            a.c0 = S.c0;
+            a.nch = S.nch;
+            a.nmaps = nk;
+            std::memcpy(a.nq, p->nq, sizeof(a.nq));
+            a.Acoef = p->Acoef;
+            a.Om = p->Om;
+            a.Stm = p->Stm;
+            a.Ste = p->Ste;
+            a.G = p->Ga + p->ga_off[j];
+            a.Gs = p->ga_stride[j];
+            a.dexp = p->sp_dexp + S.dexp_off;
+            a.fexp = p->sp_fexp;
+            a.fdig = p->sp_fdig;
+            a.Tg = p->sp_Tg;
+            a.tiles = S.tiles;
+            a.ntiles = S.ntiles;
+            a.err = p->sp_err;
+            {
+                KernelTimer kt(p, S2DWC_KIND_LWALK, s);
+                if ((st = launch_split(a, s))) return st;
+            }
+            for (int k = 0; k < nk; k++) {
+                CztArgs ca{};
+                ca.mode = p->ana_beta_mode[j];
+                ca.bl = bl;
+                ca.N = p->N;
+                ca.NP = p->NP;
+                std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
+                ca.rows = p->N * bl;
+                ca.czt = p->czt[j][ca.mode];
+                ca.tw = p->tw.at(ca.czt.M);
+                ca.in_c = p->sp_Tg + (long long)k * p->N * bl * bl;
+                ca.out_c = p->sp_Tb;
+                {
+                    KernelTimer kt(p, S2DWC_KIND_ANA_BETA, s);
+                    if ((st = launch_czt(ca, s))) return st;
+                }
+                ca.mode = CZT_ANA_ALPHA;
+                ca.czt = p->czt[j][CZT_ANA_ALPHA];
+                ca.tw = p->tw.at(ca.czt.M);
+                ca.in_c = p->sp_Tb;
+                ca.out_c = nullptr;
+                ca.out_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
+                {
+                    KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, s);
+                    if ((st = launch_czt(ca, s))) return st;
+                }
+            }
+        }
+        for (int k = 0; k < nk; k++) {
+            KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+            if ((st = launch_scoeff_copy(d_scoeff ? d_scoeff + (g0 + k) * bs2 : nullptr, d_flm + (g0 + k) * B2, p->B,
+                                         p->bl_scoeff, s)))
+                return st;
+        }
+    }
+    return S2DWC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -639,7 +814,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     *plan = nullptr;
     int st = validate_sizes(B, N, alpha, J);
     if (st) return st;
-    if (form != S2DWC_FORM_FP64) return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
+    if (form != S2DWC_FORM_FP64 && form != S2DWC_FORM_SPLIT)
+        return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
     int ndev = 0;
     S2DW_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev)
@@ -742,6 +918,7 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
     S2DW_CUDA_TRY(cudaDeviceSynchronize());
     p->bl_scoeff = bl_scoeff;
     p->tables_set = true;
+    p->sp_dexp_valid = false;
     return S2DWC_OK;
 }
 
@@ -810,8 +987,63 @@ int s2dwc_plan_analysis(s2dwc_plan *p, double *d_wav, double *d_scoeff, const do
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis: null pointer");
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis: tables not set");
     DeviceGuard dg(p->device);
+    if (p->form == S2DWC_FORM_SPLIT)
+        return run_analysis_split(p, 1, d_wav, reinterpret_cast<double2 *>(d_scoeff),
+                                  reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
     return run_analysis(p, d_wav, reinterpret_cast<double2 *>(d_scoeff),
                         reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
+}
+
+int s2dwc_plan_analysis_batch(s2dwc_plan *p, int nmaps, double *d_wav, double *d_scoeff, const double *d_flm,
+                              void *stream)
+{
+    if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_batch: null pointer");
+    if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_batch: nmaps=%d", nmaps);
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis_batch: tables not set");
+    DeviceGuard dg(p->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (p->form == S2DWC_FORM_SPLIT)
+        return run_analysis_split(p, nmaps, d_wav, reinterpret_cast<double2 *>(d_scoeff),
+                                  reinterpret_cast<const double2 *>(d_flm), s);
+    const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
+    const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
+    for (int k = 0; k < nmaps; k++) {
+        int st = run_analysis(p, d_wav + k * wtot, d_scoeff ? reinterpret_cast<double2 *>(d_scoeff) + k * bs2 : nullptr,
+                              reinterpret_cast<const double2 *>(d_flm) + k * B2, s);
+        if (st) return st;
+    }
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const double *d_wav, const double *d_scoeff,
+                               void *stream)
+{
+    if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
+        return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: null pointer");
+    if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: nmaps=%d", nmaps);
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis_batch: tables not set");
+    DeviceGuard dg(p->device);
+    const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
+    const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
+    for (int k = 0; k < nmaps; k++) {
+        int st = run_synthesis(p, reinterpret_cast<double2 *>(d_flm) + k * B2, d_wav + k * wtot,
+                               d_scoeff ? reinterpret_cast<const double2 *>(d_scoeff) + k * bs2 : nullptr,
+                               (cudaStream_t)stream);
+        if (st) return st;
+    }
+    return S2DWC_OK;
+}
+
+int s2dwc_plan_check(s2dwc_plan *p)
+{
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_check: null plan");
+    if (!p->sp_err) return S2DWC_OK;
+    DeviceGuard dg(p->device);
+    int h = 0;
+    S2DW_CUDA_TRY(cudaMemcpy(&h, p->sp_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return set_error(S2DWC_ERROR_CUDA, "a split-form kernel gave up waiting for its tensor-core pipeline");
+    return S2DWC_OK;
 }
 
 int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, const double *d_scoeff, void *stream)

@@ -1,0 +1,735 @@
+// Split-precision analysis contraction on the tcgen05 tensor cores (sm_100a).
+//
+// The analysis contraction of one scale (s2dw_core_mod.f90:625-673),
+//
+//   T^k(m, m', +-n) = sum_{l in (bl_lo, bl)} f^k(l, m) * v(l; m', m, n) * (+-1)^l,
+//   v(l; m', m, n)  = d^l_{m'm}(pi/2) d^l_{m'n}(pi/2) K_j(l) s(l, n),
+//
+// is, for a batch of maps k sharing (B, N, alpha, J), a GEMM over l whose
+// left operand v does not depend on the map: rows (m', n, +-) for one m,
+// columns (k, re/im).  Each CTA owns one m, CH consecutive m' ("chains") and
+// up to 32 maps.  Per chunk of 32 values of l:
+//
+//   * one or two walker warps advance the FP64 l-recurrence of d^l_{m'm}
+//     (one chain per lane, the recurrence of the FP64 kernel) and write the
+//     true-scale values v to shared memory;
+//   * all threads cut every value into 6 byte digits of a 48-bit fixed-point
+//     integer with a per-row power-of-two scale (two's complement bytes: five
+//     unsigned digits and a signed top digit) and store them in the K-major
+//     no-swizzle operand layout;
+//   * the map operand (f^k(l, m), cut the same way by fdig_kernel, one scale
+//     per (m, k, re/im) column) arrives by a bulk copy;
+//   * one thread issues 28 tcgen05.mma.kind::i8 (M=128, N=64, K=32): the
+//     digit products of significance level t = (5-i)+(5-j) <= 6, each level
+//     into its own int32 TMEM accumulator, so every product is summed exactly.
+//
+// The epilogue reads the seven level accumulators, combines them in FP64 with
+// the row and column scales, and applies the +-n phases and the gamma DFT of
+// the FP64 kernel (s2dw_core_mod.f90:679-705), writing Tg^k(g, m, m').
+//
+// The per-row scales come from dexp_kernel, a pre-pass that runs the same
+// walker and records the exponent of max_l |v|: the digits of every row then
+// use its full 48 bits.  The dropped products (levels 7..10) and the digit
+// truncation leave a relative error of ~1e-14 of max|T| (~1e-11 of max|w|
+// per scale at bl = 1024).
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+
+#include "s2dw_internal.h"
+
+namespace s2dw {
+namespace split {
+
+constexpr int MAPS = 32;            // maps per CTA (N = 64 columns: re, im)
+constexpr int COLS = 2 * MAPS;
+constexpr int ROWS = 128;           // M
+constexpr int DIG = 6;              // byte digits per operand
+constexpr int LEV = 7;              // significance levels kept
+constexpr int KC = 32;              // l per chunk: one K step of kind::i8
+constexpr int FIX = 8 * DIG - 1;    // digits hold rint(x * 2^(FIX - E)), |x| < 2^E
+// T = 2^(Ed + Ef - SHIFT) * sum_t C_t 2^(-8t)
+constexpr int SHIFT = 2 * FIX - 16 * (DIG - 1);
+constexpr int A_TILE = ROWS * KC;   // bytes per digit of the v operand
+constexpr int B_TILE = COLS * KC;   // bytes per digit of the map operand
+constexpr int TMEM_COLS = 512;
+constexpr int E_ZERO = -32000;      // exponent of an all-zero row or column
+constexpr int E_MIN = -960;         // rows or columns below 2^E_MIN count as zero
+constexpr int THREADS = 128;
+
+// Chains per CTA: 2*NP rows per chain (n and +-), 128 rows, chains a multiple
+// of 16 so that every staged table row starts on a 128-byte boundary.
+__host__ __device__ constexpr int chains(int NP) { return NP == 1 ? 64 : (NP == 2 ? 32 : 16); }
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// z * i^k
+__device__ __forceinline__ double2 c_ipow(double2 z, int k)
+{
+    switch (k & 3) {
+    case 0: return z;
+    case 1: return make_double2(-z.y, z.x);
+    case 2: return make_double2(-z.x, -z.y);
+    default: return make_double2(z.y, -z.x);
+    }
+}
+__device__ __forceinline__ double wmax(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int wmax_i(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// The l-walk of one chain (m', m): the recurrence of lwalk_kernel, in the same
+// arithmetic order, so that dexp_kernel and split_kernel see identical values.
+// Kw is warp-uniform (the scaled domain of chains whose start underflows).
+// ---------------------------------------------------------------------------
+struct Chain {
+    double e, ep, st;
+    int l0, Kw;
+};
+
+// All 32 lanes of the warp call this (lanes without a chain pass valid=false).
+__device__ __forceinline__ Chain chain_init(const int32_t *Ste, const double *Stm, int B, int m, int mp, bool valid)
+{
+    Chain c;
+    c.e = 0.0;
+    c.ep = 0.0;
+    c.st = 0.0;
+    c.l0 = valid ? max(mp, m) : INT_MAX;
+    int maxe = valid ? (int)Ste[(size_t)max(mp, m) * B + min(mp, m)] : INT_MIN;
+    maxe = wmax_i(maxe);
+    c.Kw = (maxe != INT_MIN && maxe < S2DW_SCALE_EXP) ? -maxe : 0;
+    if (valid) {
+        const size_t o = (size_t)c.l0 * B + min(mp, m);
+        double v = ldexp(Stm[o], (int)Ste[o] + c.Kw);
+        if (mp >= m && ((mp - m) & 1)) v = -v;
+        c.st = v;
+    }
+    return c;
+}
+
+// Value w(l) = d^l_{m'm} / Om_l(m') (true scale, Kw removed) at row l, then
+// one step to l+1.  am = a_m(l), ap = a_{m'}(l), om = Om_l(m).
+__device__ __forceinline__ double chain_step(Chain &c, int l, double am, double ap, double om)
+{
+    if (l == c.l0) c.e = c.st;
+    const double cur = c.e * om;
+    const double w = (c.Kw == 0) ? cur : ldexp(cur, -c.Kw);
+    const double en = fma(-(am * ap), c.e, -c.ep);
+    c.ep = c.e;
+    c.e = en;
+    return w;
+}
+
+// Called by all lanes after the step of row l when (l & 15) == 15.
+__device__ __forceinline__ void chain_renorm(Chain &c)
+{
+    if (c.Kw > 0) {
+        const double mx = wmax(fmax(fabs(c.e), fabs(c.ep)));
+        if (mx > ldexp(1.0, S2DW_RENORM_EXP)) {
+            const int R = min(S2DW_RENORM_EXP, c.Kw);
+            const double f = ldexp(1.0, -R);
+            c.e *= f;
+            c.ep *= f;
+            c.Kw -= R;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-point digits
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double digit_factor(int E) { return E > E_MIN ? ldexp(1.0, FIX - E) : 0.0; }
+
+__device__ __forceinline__ long long to_fixed(double x, double factor)
+{
+    long long X = __double2ll_rn(x * factor);
+    const long long lim = 1LL << FIX;
+    X = X > lim - 1 ? lim - 1 : X;
+    X = X < -lim ? -lim : X;
+    return X;
+}
+
+// Byte d (0..DIG-1) of four fixed-point integers, packed into one word.
+__device__ __forceinline__ uint32_t pack4(const long long *X, int d)
+{
+    const int sh = d < 4 ? 0 : 32;
+    const uint32_t s0 = (uint32_t)(X[0] >> sh), s1 = (uint32_t)(X[1] >> sh), s2 = (uint32_t)(X[2] >> sh),
+                   s3 = (uint32_t)(X[3] >> sh);
+    const int b = d & 3;
+    const uint32_t sel = (uint32_t)(b | ((b + 4) << 4));
+    return __byte_perm(__byte_perm(s0, s1, sel), __byte_perm(s2, s3, sel), 0x5410);
+}
+
+// 16 consecutive K values of one operand row -> the 16-byte K-half of each of
+// the DIG digit tiles.  `base` is the row's K-half inside digit tile 0;
+// consecutive digit tiles are `tile` bytes apart.
+__device__ __forceinline__ void store_digits(unsigned char *base, int tile, const long long *X)
+{
+#pragma unroll
+    for (int d = 0; d < DIG; d++) {
+        uint4 v;
+        v.x = pack4(X + 0, d);
+        v.y = pack4(X + 4, d);
+        v.z = pack4(X + 8, d);
+        v.w = pack4(X + 12, d);
+        *reinterpret_cast<uint4 *>(base + d * tile) = v;
+    }
+}
+
+// Offset of (row r, K-half kh) in a K-major no-swizzle tile of R rows x 32
+// bytes: 8-row core matrices of 128 contiguous bytes (SBO = 128), the two
+// 16-byte K halves R*16 bytes apart (LBO).
+__host__ __device__ constexpr int tile_off(int R, int r, int kh) { return kh * R * 16 + (r >> 3) * 128 + (r & 7) * 16; }
+
+// ---------------------------------------------------------------------------
+// PTX wrappers: mbarrier, bulk copy, tcgen05
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase with `parity` to complete; gives up after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (gtimer() - t0 > limit_ns) return false;
+    }
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, no-swizzle shared-memory matrix descriptor (sm_100 format:
+// start >> 4 in bits 0-13, LBO >> 4 in 16-29, SBO >> 4 in 32-45, version 1 in
+// 46-47, base offset 0, layout type 0 = no swizzle in 61-63).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::i8: S32 accumulator (bits 4-5 = 2), A and B
+// format (bits 7-9, 10-12: 0 = u8, 1 = s8), both K-major, N >> 3 in bits
+// 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_i8(int a_signed, int b_signed, int M, int N)
+{
+    return (2u << 4) | ((uint32_t)a_signed << 7) | ((uint32_t)b_signed << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on every wait
+
+// ---------------------------------------------------------------------------
+// dexp_kernel: exponent of max_{l in (blo, bl)} |v(l; m', m, n_q)| per
+// (m, m', q).  One CTA per (m, chain tile), one lane per chain.
+// ---------------------------------------------------------------------------
+template <int NP>
+__global__ void __launch_bounds__(64) dexp_kernel(SplitArgs a)
+{
+    constexpr int CH = chains(NP);
+    const int2 tile = a.tiles[blockIdx.x];
+    const int m = tile.x, p0 = tile.y * CH;
+    const int ch = threadIdx.x, mp = p0 + ch;
+    const bool valid = ch < CH && mp < a.bl;
+    Chain c = chain_init(a.Ste, a.Stm, a.B, m, mp, valid);
+    double mx[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++) mx[q] = 0.0;
+    const int lw = max(m, p0);
+    const int mpc = min(mp, a.Bp - 1);
+#pragma unroll 4
+    for (int l = lw; l < a.bl; l++) {
+        const double am = a.Acoef[(size_t)l * a.Bp + m], ap = a.Acoef[(size_t)l * a.Bp + mpc];
+        const double om = a.Om[(size_t)l * a.Bp + m];
+        const double w = chain_step(c, l, am, ap, om);
+        if (l > a.blo && valid) {
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                const double v = w * a.G[((size_t)(l - a.blo - 1) * NP + q) * a.Gs + mp];
+                mx[q] = fmax(mx[q], fabs(v));
+            }
+        }
+        if ((l & 15) == 15) chain_renorm(c);
+    }
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < NP; q++)
+            a.dexp[((size_t)m * a.bl + mp) * NP + q] = (int16_t)(mx[q] > 0.0 ? ilogb(mx[q]) + 1 : E_ZERO);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fdig_kernel: digits of the map operand for one scale.  One CTA per m;
+// column col = 2k + (0: re, 1: im).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(THREADS) fdig_kernel(FdigArgs a)
+{
+    __shared__ int sE[COLS];
+    const int m = blockIdx.x, t = threadIdx.x;
+    const int col = t >> 1, half = t & 1, k = col >> 1, comp = col & 1;
+    const int lbeg = max(a.blo + 1, m);
+    const double *f = reinterpret_cast<const double *>(a.flm) + (size_t)k * a.B * a.B * 2 + (size_t)a.B * m * 2 + comp;
+    double mx = 0.0;
+    if (k < a.nmaps)
+        for (int l = lbeg + ((lbeg & 1) ^ half); l < a.bl; l += 2) mx = fmax(mx, fabs(f[2 * (size_t)l]));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    const int E = mx > 0.0 ? ilogb(mx) + 1 : E_ZERO;
+    if (half == 0) {
+        sE[col] = E;
+        a.fexp[(size_t)m * COLS + col] = E;
+    }
+    __syncthreads();
+    const double factor = digit_factor(sE[col]);
+    const int kh = half;
+    for (int ci = 0; ci < a.nch; ci++) {
+        const int lb = (a.c0 + ci) * KC + 16 * kh;
+        long long X[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int l = lb + i;
+            const double v = (k < a.nmaps && l >= lbeg && l < a.bl) ? f[2 * (size_t)l] : 0.0;
+            X[i] = to_fixed(v, factor);
+        }
+        unsigned char *dst = a.fdig + ((size_t)m * a.nch + ci) * DIG * B_TILE + tile_off(COLS, col, kh);
+        store_digits(dst, B_TILE, X);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// split_kernel
+// ---------------------------------------------------------------------------
+template <int NP>
+struct SplitSmem {
+    static constexpr int CH = chains(NP);
+    static constexpr int WCH = CH;                    // staged lanes per table row
+    static constexpr int GEN = 0;                     // 2 stages x DIG x A_TILE
+    static constexpr int MAP = GEN + 2 * DIG * A_TILE;  // 2 stages x DIG x B_TILE
+    static constexpr int VB = MAP + 2 * DIG * B_TILE;   // values [pair*33 + li]
+    static constexpr int VB_BYTES = 64 * 33 * 8;
+    // staged tables per buffer (doubles): Ap[KC][WCH], G[KC][NP][WCH], Am[KC], Om[KC]
+    static constexpr int T_AP = 0, T_G = KC * WCH, T_AM = T_G + KC * NP * WCH, T_OM = T_AM + KC;
+    static constexpr int T_DBL = T_OM + KC;
+    static constexpr int TAB = VB + VB_BYTES;
+    static constexpr int PH = TAB + 2 * T_DBL * 8;     // phases [g*16 + n+N-1]
+    static constexpr int EF = PH + 8 * 16 * 16;        // column exponents
+    static constexpr int BAR = EF + COLS * 4;          // full[2], done[2]
+    static constexpr int TM = BAR + 4 * 8;             // TMEM base address
+    static constexpr int ABORT = TM + 8;
+    static constexpr int BYTES = ABORT + 8 + 1024;     // + alignment slack
+    static_assert(ROWS * 33 * 8 <= 2 * DIG * A_TILE + 2 * DIG * B_TILE, "epilogue tile fits the operand buffers");
+    static_assert(LEV * COLS <= TMEM_COLS, "level accumulators fit TMEM");
+};
+
+template <int NP>
+__global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
+{
+    using S = SplitSmem<NP>;
+    constexpr int CH = S::CH;
+    constexpr int PAIRS = CH * NP;  // <= 64
+    extern __shared__ unsigned char smraw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    double *vbuf = reinterpret_cast<double *>(sm + S::VB);
+    double2 *sPh = reinterpret_cast<double2 *>(sm + S::PH);
+    int *sEf = reinterpret_cast<int *>(sm + S::EF);
+    uint32_t *sTm = reinterpret_cast<uint32_t *>(sm + S::TM);
+    volatile int *sAbort = reinterpret_cast<volatile int *>(sm + S::ABORT);
+    const uint32_t bar0 = smem_u32(sm + S::BAR);
+    auto full = [&](int s) { return bar0 + 8 * s; };
+    auto done = [&](int s) { return bar0 + 16 + 8 * s; };
+
+    const int t = threadIdx.x, warp = t >> 5;
+    const int2 tile = a.tiles[blockIdx.x];
+    const int m = tile.x, p0 = tile.y * CH;
+    const int bl = a.bl, blo = a.blo, N = a.N;
+    const int lw = max(m, p0);                          // first row any chain walks
+    const int lk = max(blo + 1, lw);                    // first row with output
+    const int cw0 = lw / KC, c_last = (bl - 1) / KC;
+    const int c_start = lk / KC;
+    const bool has_mma = lk < bl;
+
+    // ---- setup: barriers, TMEM, phases, column exponents
+    if (t == 0) {
+        for (int i = 0; i < 4; i++) mbar_init(bar0 + 8 * i, 1);
+        mbar_fence_init();
+        *sAbort = 0;
+    }
+    if (warp == 0) {
+        tmem_alloc(smem_u32(sTm), TMEM_COLS);
+        tmem_relinquish();
+    }
+    for (int i = t; i < N * (2 * N - 1); i += THREADS) {
+        const int g = i / (2 * N - 1), n = i % (2 * N - 1) - (N - 1);
+        double sn, cs;
+        sincospi((double)(n * g) / (double)N, &sn, &cs);
+        sPh[g * 16 + n + N - 1] = make_double2(cs, sn);
+    }
+    if (t < COLS) sEf[t] = a.fexp[(size_t)m * COLS + t];
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *sTm;
+
+    // per-thread digit row pair (also the epilogue row t)
+    const int pair = t >> 1, kh = t & 1;
+    const int pch = pair / NP, pq = pair % NP, pmp = p0 + pch;
+    const bool prow = pair < PAIRS && pmp < bl;
+    const int Ed = prow ? (int)a.dexp[((size_t)m * bl + pmp) * NP + pq] : E_ZERO;
+    const double dfac = digit_factor(Ed);
+
+    // walker lanes
+    const bool walker = t < CH;  // warps 0 (and 1 when CH = 64)
+    const int wmp = p0 + t;
+    Chain ch;
+    if (warp < (CH + 31) / 32) ch = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
+
+    // map-operand bulk copies (thread 0): chunk c -> stage (c - c_start) & 1
+    auto issue_map_copy = [&](int c) {
+        const int st = (c - c_start) & 1;
+        mbar_expect_tx(full(st), DIG * B_TILE);
+        bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
+                 a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
+    };
+    if (t == 0 && has_mma) issue_map_copy(c_start);
+
+    // staged tables for chunk c -> buffer b
+    auto stage_tables = [&](int c, int b) {
+        double *T = reinterpret_cast<double *>(sm + S::TAB) + b * S::T_DBL;
+        const int lb = c * KC;
+        constexpr int V = S::WCH / 2;  // 16-byte pieces per row
+        for (int i = t; i < KC * V; i += THREADS) {
+            const int li = i / V, x = 2 * (i % V), l = lb + li;
+            double *d = T + S::T_AP + li * S::WCH + x;
+            if (l < bl && p0 + x < a.Bp) cp_async16(d, a.Acoef + (size_t)l * a.Bp + p0 + x);
+            else { d[0] = 0.0; d[1] = 0.0; }
+        }
+        for (int i = t; i < KC * NP * V; i += THREADS) {
+            const int li = i / (NP * V), r = i % (NP * V), q = r / V, x = 2 * (r % V), l = lb + li;
+            double *d = T + S::T_G + (li * NP + q) * S::WCH + x;
+            if (l < bl && l > blo && p0 + x < a.Gs)
+                cp_async16(d, a.G + ((size_t)(l - blo - 1) * NP + q) * a.Gs + p0 + x);
+            else { d[0] = 0.0; d[1] = 0.0; }
+        }
+        for (int i = t; i < 2 * KC; i += THREADS) {
+            const int li = i % KC, l = lb + li;
+            double *d = T + (i < KC ? S::T_AM : S::T_OM) + li;
+            const double *src = (i < KC ? a.Acoef : a.Om) + (size_t)l * a.Bp + m;
+            if (l < bl) cp_async8(d, src);
+            else *d = 0.0;
+        }
+    };
+
+    bool ok = true;
+    bool first_lev[LEV];
+#pragma unroll
+    for (int i = 0; i < LEV; i++) first_lev[i] = true;
+
+    if (has_mma) {
+        stage_tables(cw0, 0);
+        cp_commit_all();
+        cp_wait_all();
+        __syncthreads();
+        for (int c = cw0; c <= c_last; c++) {
+            const int tb = (c - cw0) & 1;
+            if (c + 1 <= c_last) stage_tables(c + 1, tb ^ 1);
+            cp_commit_all();
+            const double *T = reinterpret_cast<const double *>(sm + S::TAB) + tb * S::T_DBL;
+            const bool out = c >= c_start;
+            // ---- walk
+            if (warp < (CH + 31) / 32) {
+                const int lb = c * KC;
+                for (int li = 0; li < KC; li++) {
+                    const int l = lb + li;
+                    double vq[NP];
+#pragma unroll
+                    for (int q = 0; q < NP; q++) vq[q] = 0.0;
+                    if (l >= lw && l < bl) {
+                        const double w = chain_step(ch, l, T[S::T_AM + li], walker ? T[S::T_AP + li * S::WCH + t] : 0.0,
+                                                    T[S::T_OM + li]);
+                        if (l > blo && walker) {
+#pragma unroll
+                            for (int q = 0; q < NP; q++) vq[q] = w * T[S::T_G + (li * NP + q) * S::WCH + t];
+                        }
+                        if ((l & 15) == 15) chain_renorm(ch);
+                    }
+                    if (out && walker) {
+#pragma unroll
+                        for (int q = 0; q < NP; q++) vbuf[(t * NP + q) * 33 + li] = vq[q];
+                    }
+                }
+            }
+            __syncthreads();
+            if (out) {
+                const int gs = (c - c_start) & 1;
+                // ---- digits of rows 2*pair (+) and 2*pair+1 (-)
+                unsigned char *gen = sm + S::GEN + gs * DIG * A_TILE;
+                long long X[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) X[i] = to_fixed(prow ? vbuf[pair * 33 + 16 * kh + i] : 0.0, dfac);
+                store_digits(gen + tile_off(ROWS, 2 * pair, kh), A_TILE, X);
+#pragma unroll
+                for (int i = 1; i < 16; i += 2) X[i] = -X[i];  // (-1)^l, l = 32c + 16kh + i
+                store_digits(gen + tile_off(ROWS, 2 * pair + 1, kh), A_TILE, X);
+                fence_async_smem();
+                __syncthreads();
+                if (t == 0) {
+                    if (c + 1 <= c_last) {
+                        if (c > c_start) ok = ok && mbar_wait(done(gs ^ 1), ((c - 1 - c_start) >> 1) & 1, WAIT_NS);
+                        if (ok) issue_map_copy(c + 1);
+                    }
+                    ok = ok && mbar_wait(full(gs), ((c - c_start) >> 1) & 1, WAIT_NS);
+                    if (ok) {
+                        tc_fence_after();
+                        const uint32_t ga = smem_u32(gen), ma = smem_u32(sm + S::MAP + gs * DIG * B_TILE);
+#pragma unroll
+                        for (int i = 0; i < DIG; i++)
+#pragma unroll
+                            for (int j = 0; j < DIG; j++) {
+                                const int lev = 2 * (DIG - 1) - i - j;
+                                if (lev >= LEV) continue;
+                                const uint64_t da = smem_desc(ga + i * A_TILE, ROWS * 16, 128);
+                                const uint64_t db = smem_desc(ma + j * B_TILE, COLS * 16, 128);
+                                mma_i8(tmem + lev * COLS, da, db, idesc_i8(i == DIG - 1, j == DIG - 1, ROWS, COLS),
+                                       first_lev[lev] ? 0u : 1u);
+                                first_lev[lev] = false;
+                            }
+                        mma_commit(done(gs));
+                    } else {
+                        *sAbort = 1;
+                    }
+                }
+            }
+            cp_wait_all();
+            __syncthreads();
+            if (*sAbort) break;
+        }
+        // ---- drain: the last chunk's MMAs (the one before it was waited on
+        // when its successor was issued)
+        if (t == 0 && !*sAbort) {
+            const int cl = c_last;
+            if (!mbar_wait(done((cl - c_start) & 1), ((cl - c_start) >> 1) & 1, WAIT_NS)) *sAbort = 1;
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+
+    const bool abort = *sAbort != 0;
+    if (abort && t == 0) atomicExch(a.err, 1);
+
+    // ---- epilogue: two halves of 32 columns (16 maps)
+    double *Ts = reinterpret_cast<double *>(sm + S::GEN);  // [row * 33 + col]
+    const int ev = (N % 2 == 0) ? 1 : 0;
+    for (int h = 0; h < 2; h++) {
+        for (int blk = 0; blk < 2; blk++) {
+            const int col0 = 32 * h + 16 * blk;
+            double acc[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) acc[i] = 0.0;
+            if (has_mma && !abort) {
+#pragma unroll 1
+                for (int lev = 0; lev < LEV; lev++) {
+                    int32_t r[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + lev * COLS + col0, r);
+                    const double wgt = ldexp(1.0, -8 * lev);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int Ef = sEf[col0 + i];
+                const bool z = Ed <= E_MIN || Ef <= E_MIN;
+                Ts[t * 33 + 16 * blk + i] = z ? 0.0 : ldexp(acc[i], Ed + Ef - SHIFT);
+            }
+        }
+        __syncthreads();
+        // (chain, map) items of this half
+        constexpr int ITEMS = CH * 16;
+        for (int it = t; it < ITEMS; it += THREADS) {
+            const int c = it % CH, kk = it / CH, k = 16 * h + kk, mp = p0 + c;
+            if (mp >= bl || k >= a.nmaps) continue;
+            double2 Tp[NP], Tm[NP];
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                const int n = a.nq[q], pr = c * NP + q;
+                const double2 sum = make_double2(Ts[(2 * pr) * 33 + 2 * kk], Ts[(2 * pr) * 33 + 2 * kk + 1]);
+                const double2 dif = make_double2(Ts[(2 * pr + 1) * 33 + 2 * kk], Ts[(2 * pr + 1) * 33 + 2 * kk + 1]);
+                if (n == 0) {
+                    Tp[q] = c_ipow(sum, -m);
+                    Tm[q] = make_double2(0.0, 0.0);
+                } else {
+                    Tp[q] = c_ipow(sum, n - m - ev);
+                    double2 x = c_ipow(dif, -n - m + ev);
+                    if ((mp + n) & 1) x = make_double2(-x.x, -x.y);
+                    Tm[q] = x;
+                }
+            }
+            double2 *out = a.Tg + (size_t)k * N * bl * bl;
+            for (int g = 0; g < N; g++) {
+                double2 y = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < NP; q++) {
+                    const int n = a.nq[q];
+                    y = c_add(y, c_mul(Tp[q], sPh[g * 16 + n + N - 1]));
+                    if (n != 0) y = c_add(y, c_mul(Tm[q], sPh[g * 16 - n + N - 1]));
+                }
+                out[((size_t)g * bl + m) * bl + mp] = y;
+            }
+        }
+        __syncthreads();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
+}
+
+}  // namespace split
+
+int split_chains(int NP) { return split::chains(NP); }
+int split_maps_per_pass() { return split::MAPS; }
+long long split_fdig_bytes(int bl, int nch) { return (long long)bl * nch * split::DIG * split::B_TILE; }
+
+int launch_split_dexp(const SplitArgs &a, cudaStream_t s)
+{
+    if (a.ntiles <= 0) return S2DWC_OK;
+    const int thr = split::chains(a.NP) > 32 ? 64 : 32;
+    switch (a.NP) {
+    case 1: split::dexp_kernel<1><<<a.ntiles, thr, 0, s>>>(a); break;
+    case 2: split::dexp_kernel<2><<<a.ntiles, thr, 0, s>>>(a); break;
+    case 3: split::dexp_kernel<3><<<a.ntiles, thr, 0, s>>>(a); break;
+    default: split::dexp_kernel<4><<<a.ntiles, thr, 0, s>>>(a); break;
+    }
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_split_fdig(const FdigArgs &a, cudaStream_t s)
+{
+    if (a.bl <= 0 || a.nch <= 0) return S2DWC_OK;
+    split::fdig_kernel<<<a.bl, split::THREADS, 0, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+template <int NP>
+static int launch_split_t(const SplitArgs &a, cudaStream_t s)
+{
+    const int bytes = split::SplitSmem<NP>::BYTES;
+    static bool attr = false;
+    if (!attr) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(split::split_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        attr = true;
+    }
+    split::split_kernel<NP><<<a.ntiles, split::THREADS, bytes, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_split(const SplitArgs &a, cudaStream_t s)
+{
+    if (a.ntiles <= 0) return S2DWC_OK;
+    switch (a.NP) {
+    case 1: return launch_split_t<1>(a, s);
+    case 2: return launch_split_t<2>(a, s);
+    case 3: return launch_split_t<3>(a, s);
+    default: return launch_split_t<4>(a, s);
+    }
+}
+
+}  // namespace s2dw

@@ -16,13 +16,17 @@ from .core import band_limits
 
 
 class Plan:
-    def __init__(self, B, N, alpha, J, device=0):
+    FP64, SPLIT = 0, 1
+
+    def __init__(self, B, N, alpha, J, device=0, form=0):
         import torch
 
         self.B, self.N, self.alpha, self.J, self.device = int(B), int(N), float(alpha), int(J), int(device)
+        self.form = int(form)
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            check(lib().s2dwc_plan_create(ctypes.byref(h), self.B, self.N, self.alpha, self.J, 0, self.device))
+            check(lib().s2dwc_plan_create(ctypes.byref(h), self.B, self.N, self.alpha, self.J, self.form,
+                                          self.device))
         self._h = h
         offs = (ctypes.c_longlong * (J + 2))()
         check(lib().s2dwc_plan_wav_offsets(self._h, offs))
@@ -120,6 +124,31 @@ class Plan:
                                                 self._ptr(scoeff, torch.complex128, self.bl_scoeff ** 2),
                                                 self._ptr(flm, torch.complex128, self.B * self.B),
                                                 self._stream(stream)))
+
+    def analysis_batch(self, flm, wav, scoeff, stream=None):
+        """Analysis of flm.shape[0] maps: flm (n, B, B) complex128 (each map
+        stored as the reference's column-major flm), wav (n, wav_size), scoeff
+        (n, bl_scoeff**2)."""
+        import torch
+
+        n = int(flm.shape[0])
+        check(lib().s2dwc_plan_analysis_batch(self._h, n, self._ptr(wav, torch.float64, n * self.wav_size),
+                                              self._ptr(scoeff, torch.complex128, n * self.bl_scoeff ** 2),
+                                              self._ptr(flm, torch.complex128, n * self.B * self.B),
+                                              self._stream(stream)))
+
+    def synthesis_batch(self, wav, scoeff, flm, stream=None):
+        import torch
+
+        n = int(flm.shape[0])
+        check(lib().s2dwc_plan_synthesis_batch(self._h, n, self._ptr(flm, torch.complex128, n * self.B * self.B),
+                                               self._ptr(wav, torch.float64, n * self.wav_size),
+                                               self._ptr(scoeff, torch.complex128, n * self.bl_scoeff ** 2),
+                                               self._stream(stream)))
+
+    def check(self):
+        """Raises S2DWError if a split-form kernel gave up waiting (synchronises)."""
+        check(lib().s2dwc_plan_check(self._h))
 
     def synthesis(self, wav, scoeff, flm, stream=None):
         import torch

@@ -1,0 +1,80 @@
+"""Split-precision analysis (tensor-core int8 digit contraction) against the
+FP64 analysis of the same maps, for batches of maps.
+
+Tolerance: per map and per scale, max|w_split - w_fp64| <= 1e-10 * max|w_fp64|
+(the split form's stated bound; its design error is ~1e-11), and the FP64
+synthesis of the split coefficients reconstructs flm within 1e-10.  Cases
+cover every size of the positive-n set (NP = 1..4), alpha = 3, a batch larger
+than one 32-map group, and a batch of one."""
+import numpy as np
+import pytest
+
+from s2dw_b200.workload import gaussian_flm, transform_setup
+
+TOL_W = 1e-10
+TOL_RECON = 1e-10
+
+
+def _run(B, N, alpha, nmaps, seed0=100):
+    import torch
+
+    from s2dw_b200.device import Plan
+
+    t = transform_setup(B, N, alpha)
+    J = t["J"]
+    plain = Plan(B, N, alpha, J)
+    split = Plan(B, N, alpha, J, form=Plan.SPLIT)
+    for p in (plain, split):
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    flms = [gaussian_flm(B, seed=seed0 + k) for k in range(nmaps)]
+    d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
+    bs2 = max(1, t["bl_scoeff"] ** 2)
+    w_ref = torch.empty((nmaps, plain.wav_size), dtype=torch.float64, device="cuda")
+    s_ref = torch.empty((nmaps, bs2), dtype=torch.complex128, device="cuda")
+    w_sp = torch.full_like(w_ref, np.nan)
+    s_sp = torch.full_like(s_ref, np.nan)
+    plain.analysis_batch(d_flm, w_ref, s_ref)
+    split.analysis_batch(d_flm, w_sp, s_sp)
+    split.check()
+    out = torch.empty_like(d_flm)
+    plain.synthesis_batch(w_sp, s_sp, out)
+    torch.cuda.synchronize()
+    wr, ws = w_ref.cpu().numpy(), w_sp.cpu().numpy()
+    offs = plain.wav_offsets
+    worst = 0.0
+    for k in range(nmaps):
+        for j in range(J + 1):
+            a, b = wr[k, offs[j]:offs[j + 1]], ws[k, offs[j]:offs[j + 1]]
+            scale = np.abs(a).max()
+            if scale == 0:
+                assert np.abs(b).max() == 0
+                continue
+            worst = max(worst, np.abs(a - b).max() / scale)
+    np.testing.assert_array_equal(s_sp.cpu().numpy(), s_ref.cpu().numpy())
+    recon = max(np.abs(out[k].cpu().numpy().T - flms[k]).max() for k in range(nmaps))
+    plain.close()
+    split.close()
+    return worst, recon
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha,nmaps", [
+    (64, 3, 2.0, 5),    # NP = 2 (n = 0, 2)
+    (64, 2, 2.0, 3),    # NP = 1
+    (48, 5, 3.0, 4),    # NP = 3
+    (64, 8, 2.0, 2),    # NP = 4
+    (32, 4, 2.0, 40),   # two map groups
+    (96, 4, 2.0, 1),    # one map
+])
+def test_split_matches_fp64(B, N, alpha, nmaps):
+    worst, recon = _run(B, N, alpha, nmaps)
+    assert worst <= TOL_W, f"max|dw|/max|w| = {worst:.3e}"
+    assert recon <= TOL_RECON, f"recon {recon:.3e}"
+
+
+@pytest.mark.gpu
+def test_split_b256_n5():
+    """The split-form comparison configuration: B=256, N=5, alpha=2."""
+    worst, recon = _run(256, 5, 2.0, 4)
+    assert worst <= TOL_W, f"max|dw|/max|w| = {worst:.3e}"
+    assert recon <= TOL_RECON, f"recon {recon:.3e}"
