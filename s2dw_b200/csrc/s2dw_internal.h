@@ -208,6 +208,7 @@ struct SplitArgs {
     const int32_t *fexp;       // [m*64 + col] exponent of the map column
     const uint8_t *fdig;       // [(m*nch + chunk)*5 + digit][2048] map digits
     double2 *Tg;               // [k][g][m][m'] per map
+    const double2 *ph;         // [g*16 + n+N-1] = exp(i pi n g / N)
     const int2 *tiles;         // (m, chain tile)
     int ntiles;
     int *err;                  // set to 1 when a wait gave up

@@ -77,7 +77,7 @@ struct s2dwc_plan {
     int16_t *sp_dexp = nullptr;
     int32_t *sp_fexp = nullptr;
     uint8_t *sp_fdig = nullptr;
-    double2 *sp_Tg = nullptr, *sp_Tb = nullptr;
+    double2 *sp_Tg = nullptr, *sp_Tb = nullptr, *sp_ph = nullptr;
     int *sp_err = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
@@ -640,6 +640,14 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             (st = dev_alloc(p, &p->sp_Tb, (size_t)p->N * 2 * b2)) || (st = dev_alloc(p, &p->sp_err, 1)))
             return st;
         S2DW_CUDA_TRY(cudaMemsetAsync(p->sp_err, 0, sizeof(int), s));
+        // gamma-DFT phases exp(i pi n g / N), [g*16 + n+N-1]
+        std::vector<double2> ph((size_t)p->N * 16, make_double2(0.0, 0.0));
+        for (int g = 0; g < p->N; g++)
+            for (int n = -(p->N - 1); n <= p->N - 1; n++) {
+                const long double x = 3.141592653589793238462643383279502884L * (long double)(n * g) / (long double)p->N;
+                ph[(size_t)g * 16 + n + p->N - 1] = make_double2((double)cosl(x), (double)sinl(x));
+            }
+        if ((st = dev_upload(p, &p->sp_ph, ph))) return st;
         p->sp_alloc = true;
     }
     if (!p->sp_dexp_valid) {
@@ -720,6 +728,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             a.fexp = p->sp_fexp;
             a.fdig = p->sp_fdig;
             a.Tg = p->sp_Tg;
+            a.ph = p->sp_ph;
             a.tiles = S.tiles;
             a.ntiles = S.ntiles;
             a.err = p->sp_err;

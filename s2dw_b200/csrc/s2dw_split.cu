@@ -96,9 +96,13 @@ __device__ __forceinline__ int wmax_i(int v)
 // Kw is warp-uniform (the scaled domain of chains whose start underflows).
 // ---------------------------------------------------------------------------
 struct Chain {
-    double e, ep, st;
+    double e, ep, st, sc;  // sc = 2^-Kw (0 when below the double range)
     int l0, Kw;
 };
+
+// 2^E for E in [-1022, 1023], built from the exponent bits.
+__device__ __forceinline__ double pow2i(int E) { return __longlong_as_double((long long)(E + 1023) << 52); }
+__device__ __forceinline__ double pow2_or_zero(int E) { return E >= -1022 ? pow2i(E) : 0.0; }
 
 // All 32 lanes of the warp call this (lanes without a chain pass valid=false).
 __device__ __forceinline__ Chain chain_init(const int32_t *Ste, const double *Stm, int B, int m, int mp, bool valid)
@@ -111,6 +115,7 @@ __device__ __forceinline__ Chain chain_init(const int32_t *Ste, const double *St
     int maxe = valid ? (int)Ste[(size_t)max(mp, m) * B + min(mp, m)] : INT_MIN;
     maxe = wmax_i(maxe);
     c.Kw = (maxe != INT_MIN && maxe < S2DW_SCALE_EXP) ? -maxe : 0;
+    c.sc = pow2_or_zero(-c.Kw);
     if (valid) {
         const size_t o = (size_t)c.l0 * B + min(mp, m);
         double v = ldexp(Stm[o], (int)Ste[o] + c.Kw);
@@ -120,13 +125,13 @@ __device__ __forceinline__ Chain chain_init(const int32_t *Ste, const double *St
     return c;
 }
 
-// Value w(l) = d^l_{m'm} / Om_l(m') (true scale, Kw removed) at row l, then
-// one step to l+1.  am = a_m(l), ap = a_{m'}(l), om = Om_l(m).
+// Value w(l) = d^l_{m'm} / Om_l(m') (true scale) at row l, then one step to
+// l+1.  am = a_m(l), ap = a_{m'}(l), om = Om_l(m).  Values below 2^-1022
+// times the walk's scale flush to zero (they are below 2^-600 of the row).
 __device__ __forceinline__ double chain_step(Chain &c, int l, double am, double ap, double om)
 {
     if (l == c.l0) c.e = c.st;
-    const double cur = c.e * om;
-    const double w = (c.Kw == 0) ? cur : ldexp(cur, -c.Kw);
+    const double w = (c.e * om) * c.sc;
     const double en = fma(-(am * ap), c.e, -c.ep);
     c.ep = c.e;
     c.e = en;
@@ -138,12 +143,13 @@ __device__ __forceinline__ void chain_renorm(Chain &c)
 {
     if (c.Kw > 0) {
         const double mx = wmax(fmax(fabs(c.e), fabs(c.ep)));
-        if (mx > ldexp(1.0, S2DW_RENORM_EXP)) {
+        if (mx > pow2i(S2DW_RENORM_EXP)) {
             const int R = min(S2DW_RENORM_EXP, c.Kw);
-            const double f = ldexp(1.0, -R);
+            const double f = pow2i(-R);
             c.e *= f;
             c.ep *= f;
             c.Kw -= R;
+            c.sc = pow2_or_zero(-c.Kw);
         }
     }
 }
@@ -151,7 +157,7 @@ __device__ __forceinline__ void chain_renorm(Chain &c)
 // ---------------------------------------------------------------------------
 // Fixed-point digits
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double digit_factor(int E) { return E > E_MIN ? ldexp(1.0, FIX - E) : 0.0; }
+__device__ __forceinline__ double digit_factor(int E) { return E > E_MIN ? pow2i(FIX - E) : 0.0; }
 
 __device__ __forceinline__ long long to_fixed(double x, double factor)
 {
@@ -397,24 +403,30 @@ __global__ void __launch_bounds__(THREADS) fdig_kernel(FdigArgs a)
 template <int NP>
 struct SplitSmem {
     static constexpr int CH = chains(NP);
-    static constexpr int WCH = CH;                    // staged lanes per table row
-    static constexpr int GEN = 0;                     // 2 stages x DIG x A_TILE
+    static constexpr int WCH = CH;                      // staged lanes per table row
+    static constexpr int GEN = 0;                       // 2 stages x DIG x A_TILE
     static constexpr int MAP = GEN + 2 * DIG * A_TILE;  // 2 stages x DIG x B_TILE
-    static constexpr int VB = MAP + 2 * DIG * B_TILE;   // values [pair*33 + li]
+    static constexpr int VB = MAP + 2 * DIG * B_TILE;   // chain values w [chain*33 + li]
     static constexpr int VB_BYTES = 64 * 33 * 8;
     // staged tables per buffer (doubles): Ap[KC][WCH], G[KC][NP][WCH], Am[KC], Om[KC]
     static constexpr int T_AP = 0, T_G = KC * WCH, T_AM = T_G + KC * NP * WCH, T_OM = T_AM + KC;
     static constexpr int T_DBL = T_OM + KC;
     static constexpr int TAB = VB + VB_BYTES;
-    static constexpr int PH = TAB + 2 * T_DBL * 8;     // phases [g*16 + n+N-1]
-    static constexpr int EF = PH + 8 * 16 * 16;        // column exponents
-    static constexpr int BAR = EF + COLS * 4;          // full[2], done[2]
-    static constexpr int TM = BAR + 4 * 8;             // TMEM base address
+    static constexpr int PH = TAB + 2 * T_DBL * 8;  // phases [g*16 + n+N-1]
+    static constexpr int EF = PH + 8 * 16 * 16;     // column scale factors 2^(Ef - SHIFT)
+    static constexpr int BAR = EF + COLS * 8;       // full[2], done[2]
+    static constexpr int TM = BAR + 4 * 8;          // TMEM base address
     static constexpr int ABORT = TM + 8;
-    static constexpr int BYTES = ABORT + 8 + 1024;     // + alignment slack
+    static constexpr int BYTES = ABORT + 8 + 1024;  // + alignment slack
     static_assert(ROWS * 33 * 8 <= 2 * DIG * A_TILE + 2 * DIG * B_TILE, "epilogue tile fits the operand buffers");
     static_assert(LEV * COLS <= TMEM_COLS, "level accumulators fit TMEM");
 };
+
+// Thread roles: warps 0 (and 1 when CH = 64) walk the chains; thread ISSUER
+// (warp 3, never a walker) issues the MMAs of the previous chunk while the
+// walkers advance, so the walk, the MMA issue and the tensor cores overlap;
+// all 128 threads stage tables, cut digits and run the epilogue.
+constexpr int ISSUER = 96;
 
 template <int NP>
 __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
@@ -422,11 +434,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
     using S = SplitSmem<NP>;
     constexpr int CH = S::CH;
     constexpr int PAIRS = CH * NP;  // <= 64
+    constexpr int NWALK = (CH + 31) / 32;
     extern __shared__ unsigned char smraw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     double *vbuf = reinterpret_cast<double *>(sm + S::VB);
     double2 *sPh = reinterpret_cast<double2 *>(sm + S::PH);
-    int *sEf = reinterpret_cast<int *>(sm + S::EF);
+    double *sFc = reinterpret_cast<double *>(sm + S::EF);
     uint32_t *sTm = reinterpret_cast<uint32_t *>(sm + S::TM);
     volatile int *sAbort = reinterpret_cast<volatile int *>(sm + S::ABORT);
     const uint32_t bar0 = smem_u32(sm + S::BAR);
@@ -437,13 +450,13 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
     const int2 tile = a.tiles[blockIdx.x];
     const int m = tile.x, p0 = tile.y * CH;
     const int bl = a.bl, blo = a.blo, N = a.N;
-    const int lw = max(m, p0);                          // first row any chain walks
-    const int lk = max(blo + 1, lw);                    // first row with output
+    const int lw = max(m, p0);        // first row any chain walks
+    const int lk = max(blo + 1, lw);  // first row with output
     const int cw0 = lw / KC, c_last = (bl - 1) / KC;
     const int c_start = lk / KC;
     const bool has_mma = lk < bl;
 
-    // ---- setup: barriers, TMEM, phases, column exponents
+    // ---- setup: barriers, TMEM, phases, column scales
     if (t == 0) {
         for (int i = 0; i < 4; i++) mbar_init(bar0 + 8 * i, 1);
         mbar_fence_init();
@@ -453,13 +466,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
         tmem_alloc(smem_u32(sTm), TMEM_COLS);
         tmem_relinquish();
     }
-    for (int i = t; i < N * (2 * N - 1); i += THREADS) {
-        const int g = i / (2 * N - 1), n = i % (2 * N - 1) - (N - 1);
-        double sn, cs;
-        sincospi((double)(n * g) / (double)N, &sn, &cs);
-        sPh[g * 16 + n + N - 1] = make_double2(cs, sn);
+    for (int i = t; i < N * 16; i += THREADS) sPh[i] = a.ph[i];
+    if (t < COLS) {
+        const int Ef = a.fexp[(size_t)m * COLS + t];
+        sFc[t] = Ef > E_MIN ? pow2i(Ef - SHIFT) : 0.0;
     }
-    if (t < COLS) sEf[t] = a.fexp[(size_t)m * COLS + t];
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -471,21 +482,56 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
     const bool prow = pair < PAIRS && pmp < bl;
     const int Ed = prow ? (int)a.dexp[((size_t)m * bl + pmp) * NP + pq] : E_ZERO;
     const double dfac = digit_factor(Ed);
+    const double rowf = Ed > E_MIN ? pow2i(Ed) : 0.0;
 
     // walker lanes
-    const bool walker = t < CH;  // warps 0 (and 1 when CH = 64)
+    const bool walker = t < CH;
     const int wmp = p0 + t;
     Chain ch;
-    if (warp < (CH + 31) / 32) ch = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
+    if (warp < NWALK) ch = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
 
-    // map-operand bulk copies (thread 0): chunk c -> stage (c - c_start) & 1
+    auto stage_of = [&](int c) { return (c - c_start) & 1; };
+    auto use_of = [&](int c) { return (uint32_t)(((c - c_start) >> 1) & 1); };
+    // map-operand bulk copy of chunk c into its stage (ISSUER or setup)
     auto issue_map_copy = [&](int c) {
-        const int st = (c - c_start) & 1;
+        const int st = stage_of(c);
         mbar_expect_tx(full(st), DIG * B_TILE);
         bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
                  a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
     };
     if (t == 0 && has_mma) issue_map_copy(c_start);
+
+    // MMAs of chunk c (ISSUER): after the MMAs of c-1 finished (their stage
+    // is the one chunk c+1 reuses), start the map copy of c+1, wait for the
+    // map digits of c, issue the digit products of levels < LEV, commit.
+    const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
+                   idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
+    bool first_lev[LEV];
+#pragma unroll
+    for (int i = 0; i < LEV; i++) first_lev[i] = true;
+    auto issue_mmas = [&](int c) -> bool {
+        const int gs = stage_of(c);
+        if (c > c_start && !mbar_wait(done(gs ^ 1), use_of(c - 1), WAIT_NS)) return false;
+        if (c + 1 <= c_last) issue_map_copy(c + 1);
+        if (!mbar_wait(full(gs), use_of(c), WAIT_NS)) return false;
+        tc_fence_after();
+        const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
+        const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
+#pragma unroll
+        for (int i = 0; i < DIG; i++)
+#pragma unroll
+            for (int j = 0; j < DIG; j++) {
+                const int lev = 2 * (DIG - 1) - i - j;
+                if (lev >= LEV) continue;
+                const uint32_t id = (i == DIG - 1) ? (j == DIG - 1 ? idesc_ss : idesc_su)
+                                                   : (j == DIG - 1 ? idesc_us : idesc_uu);
+                mma_i8(tmem + lev * COLS, da0 + (uint64_t)((i * A_TILE) >> 4), db0 + (uint64_t)((j * B_TILE) >> 4),
+                       id, first_lev[lev] ? 0u : 1u);
+                first_lev[lev] = false;
+            }
+        mma_commit(done(gs));
+        return true;
+    };
 
     // staged tables for chunk c -> buffer b
     auto stage_tables = [&](int c, int b) {
@@ -514,11 +560,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
         }
     };
 
-    bool ok = true;
-    bool first_lev[LEV];
-#pragma unroll
-    for (int i = 0; i < LEV; i++) first_lev[i] = true;
-
+    int pending = -1;  // chunk whose digits are ready and whose MMAs are not issued
     if (has_mma) {
         stage_tables(cw0, 0);
         cp_commit_all();
@@ -530,79 +572,76 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
             cp_commit_all();
             const double *T = reinterpret_cast<const double *>(sm + S::TAB) + tb * S::T_DBL;
             const bool out = c >= c_start;
-            // ---- walk
-            if (warp < (CH + 31) / 32) {
+            if (t == ISSUER && pending >= 0 && !issue_mmas(pending)) *sAbort = 1;
+            // ---- walk: chain values w(l) of this chunk, coefficients read in
+            // blocks of 8 rows so that their loads overlap the recurrence
+            if (warp < NWALK) {
                 const int lb = c * KC;
-                for (int li = 0; li < KC; li++) {
-                    const int l = lb + li;
-                    double vq[NP];
+                const int lo = max(lb, lw) - lb, hi = min(lb + KC, bl) - lb;
+                double *vrow = vbuf + t * 33;
+                if (lo == 0 && hi == KC) {
+                    // full chunk: straight-line 32 steps, values kept in
+                    // registers until the walk ends so that no store orders
+                    // the coefficient loads (renormalisation at l = 15, 31 mod 32)
+                    double wv[KC];
 #pragma unroll
-                    for (int q = 0; q < NP; q++) vq[q] = 0.0;
-                    if (l >= lw && l < bl) {
-                        const double w = chain_step(ch, l, T[S::T_AM + li], walker ? T[S::T_AP + li * S::WCH + t] : 0.0,
-                                                    T[S::T_OM + li]);
-                        if (l > blo && walker) {
-#pragma unroll
-                            for (int q = 0; q < NP; q++) vq[q] = w * T[S::T_G + (li * NP + q) * S::WCH + t];
-                        }
-                        if ((l & 15) == 15) chain_renorm(ch);
+                    for (int li = 0; li < KC; li++) {
+                        wv[li] = chain_step(ch, lb + li, T[S::T_AM + li], walker ? T[S::T_AP + li * S::WCH + t] : 0.0,
+                                            T[S::T_OM + li]);
+                        if ((li & 15) == 15) chain_renorm(ch);
                     }
                     if (out && walker) {
 #pragma unroll
-                        for (int q = 0; q < NP; q++) vbuf[(t * NP + q) * 33 + li] = vq[q];
+                        for (int li = 0; li < KC; li++) vrow[li] = wv[li];
+                    }
+                } else
+                for (int li0 = 0; li0 < KC; li0 += 8) {
+                    double am[8], ap[8], om[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        am[u] = T[S::T_AM + li0 + u];
+                        ap[u] = walker ? T[S::T_AP + (li0 + u) * S::WCH + t] : 0.0;
+                        om[u] = T[S::T_OM + li0 + u];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int li = li0 + u, l = lb + li;
+                        double w = 0.0;
+                        if (li >= lo && li < hi) {
+                            w = chain_step(ch, l, am[u], ap[u], om[u]);
+                            if ((l & 15) == 15) chain_renorm(ch);
+                        }
+                        if (out && walker) vrow[li] = w;
                     }
                 }
             }
             __syncthreads();
             if (out) {
-                const int gs = (c - c_start) & 1;
-                // ---- digits of rows 2*pair (+) and 2*pair+1 (-)
-                unsigned char *gen = sm + S::GEN + gs * DIG * A_TILE;
+                // ---- digits of rows 2*pair (+) and 2*pair+1 (-): v = w * G
+                unsigned char *gen = sm + S::GEN + stage_of(c) * DIG * A_TILE;
+                const int lb = c * KC;
                 long long X[16];
 #pragma unroll
-                for (int i = 0; i < 16; i++) X[i] = to_fixed(prow ? vbuf[pair * 33 + 16 * kh + i] : 0.0, dfac);
+                for (int i = 0; i < 16; i++) {
+                    const int li = 16 * kh + i, l = lb + li;
+                    double v = 0.0;
+                    if (prow && l > blo) v = vbuf[pch * 33 + li] * T[S::T_G + (li * NP + pq) * S::WCH + pch];
+                    X[i] = to_fixed(v, dfac);
+                }
                 store_digits(gen + tile_off(ROWS, 2 * pair, kh), A_TILE, X);
 #pragma unroll
                 for (int i = 1; i < 16; i += 2) X[i] = -X[i];  // (-1)^l, l = 32c + 16kh + i
                 store_digits(gen + tile_off(ROWS, 2 * pair + 1, kh), A_TILE, X);
                 fence_async_smem();
-                __syncthreads();
-                if (t == 0) {
-                    if (c + 1 <= c_last) {
-                        if (c > c_start) ok = ok && mbar_wait(done(gs ^ 1), ((c - 1 - c_start) >> 1) & 1, WAIT_NS);
-                        if (ok) issue_map_copy(c + 1);
-                    }
-                    ok = ok && mbar_wait(full(gs), ((c - c_start) >> 1) & 1, WAIT_NS);
-                    if (ok) {
-                        tc_fence_after();
-                        const uint32_t ga = smem_u32(gen), ma = smem_u32(sm + S::MAP + gs * DIG * B_TILE);
-#pragma unroll
-                        for (int i = 0; i < DIG; i++)
-#pragma unroll
-                            for (int j = 0; j < DIG; j++) {
-                                const int lev = 2 * (DIG - 1) - i - j;
-                                if (lev >= LEV) continue;
-                                const uint64_t da = smem_desc(ga + i * A_TILE, ROWS * 16, 128);
-                                const uint64_t db = smem_desc(ma + j * B_TILE, COLS * 16, 128);
-                                mma_i8(tmem + lev * COLS, da, db, idesc_i8(i == DIG - 1, j == DIG - 1, ROWS, COLS),
-                                       first_lev[lev] ? 0u : 1u);
-                                first_lev[lev] = false;
-                            }
-                        mma_commit(done(gs));
-                    } else {
-                        *sAbort = 1;
-                    }
-                }
+                pending = c;
             }
             cp_wait_all();
             __syncthreads();
             if (*sAbort) break;
         }
-        // ---- drain: the last chunk's MMAs (the one before it was waited on
-        // when its successor was issued)
-        if (t == 0 && !*sAbort) {
-            const int cl = c_last;
-            if (!mbar_wait(done((cl - c_start) & 1), ((cl - c_start) >> 1) & 1, WAIT_NS)) *sAbort = 1;
+        // ---- the last chunk's MMAs, then drain
+        if (t == ISSUER && !*sAbort) {
+            if (!issue_mmas(c_last) || !mbar_wait(done(stage_of(c_last)), use_of(c_last), WAIT_NS)) *sAbort = 1;
         }
         tc_fence_before();
         __syncthreads();
@@ -622,21 +661,17 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
 #pragma unroll
             for (int i = 0; i < 16; i++) acc[i] = 0.0;
             if (has_mma && !abort) {
-#pragma unroll 1
+#pragma unroll
                 for (int lev = 0; lev < LEV; lev++) {
                     int32_t r[16];
                     tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + lev * COLS + col0, r);
-                    const double wgt = ldexp(1.0, -8 * lev);
+                    const double wgt = pow2i(-8 * lev);
 #pragma unroll
                     for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const int Ef = sEf[col0 + i];
-                const bool z = Ed <= E_MIN || Ef <= E_MIN;
-                Ts[t * 33 + 16 * blk + i] = z ? 0.0 : ldexp(acc[i], Ed + Ef - SHIFT);
-            }
+            for (int i = 0; i < 16; i++) Ts[t * 33 + 16 * blk + i] = (acc[i] * rowf) * sFc[col0 + i];
         }
         __syncthreads();
         // (chain, map) items of this half
