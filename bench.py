@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=4096,
                     help="mixed request stream for the serving p50/p99 (0 = skip)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of replaying a CUDA graph")
+    ap.add_argument("--split-maps", type=int, default=32,
+                    help="maps per batch for the split-precision measurement (0: skip)")
     return ap.parse_args()
 
 
@@ -135,7 +137,7 @@ def contraction_flops_per_scale(B, N, alpha, J):
 
 
 def serving_stats(n_requests, device):
-    """configs[3]-style stream: Poisson arrivals, B uniform over
+    """The mixed serving stream: Poisson arrivals, B uniform over
     {32,...,1024}, N uniform over 1..8, alpha in {2,3}, J=Jmax, half analyses
     and half syntheses (inputs from analyses of seeded maps).  The arrival
     rate is 70% of the throughput measured with every request arriving at
@@ -170,6 +172,79 @@ def serving_stats(n_requests, device):
                "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
                          "half analysis / half synthesis, device-resident inputs, graph replay"})
     return st
+
+
+def split_stats(B, N, alpha, J, maps, repeats=3):
+    """Split-precision form on a batch of `maps` seeded maps (the form's
+    tensor-core contraction shares its d-operand across the batch): device
+    time of batched analysis+synthesis pairs per map for the split plan
+    (split analysis, FP64 synthesis) and for the FP64 plan on the same batch,
+    the serialised contraction time of each form, and the split form's worst
+    per-scale max|w_split - w_fp64| / max|w_fp64| and reconstruction error."""
+    import torch
+
+    from s2dw_b200.device import Plan
+    from s2dw_b200.workload import gaussian_flm, transform_setup
+
+    t = transform_setup(B, N, alpha, J)
+    plain = Plan(B, N, alpha, J)
+    split = Plan(B, N, alpha, J, form=Plan.SPLIT)
+    for p in (plain, split):
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    flms = [gaussian_flm(B, seed=k) for k in range(maps)]
+    d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
+    bs2 = max(1, t["bl_scoeff"] ** 2)
+    w_ref = torch.empty((maps, plain.wav_size), dtype=torch.float64, device="cuda")
+    w_sp = torch.empty_like(w_ref)
+    s_ref = torch.empty((maps, bs2), dtype=torch.complex128, device="cuda")
+    s_sp = torch.empty_like(s_ref)
+    out = torch.empty_like(d_flm)
+    plain.analysis_batch(d_flm, w_ref, s_ref)
+    split.analysis_batch(d_flm, w_sp, s_sp)
+    split.check()
+    plain.synthesis_batch(w_sp, s_sp, out)
+    torch.cuda.synchronize()
+    wr, ws = w_ref.cpu().numpy(), w_sp.cpu().numpy()
+    offs = plain.wav_offsets
+    werr = 0.0
+    for k in range(maps):
+        for j in range(J + 1):
+            a_, b_ = wr[k, offs[j]:offs[j + 1]], ws[k, offs[j]:offs[j + 1]]
+            sc = np.abs(a_).max()
+            if sc > 0:
+                werr = max(werr, float(np.abs(a_ - b_).max() / sc))
+    recon = max(float(np.abs(out[k].cpu().numpy().T - flms[k]).max()) for k in range(maps))
+    del wr, ws
+
+    def timed(ana, syn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            ana.analysis_batch(d_flm, w_sp, s_sp)
+            syn.synthesis_batch(w_sp, s_sp, out)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / repeats
+
+    t_split = timed(split, plain)
+    t_fp64 = timed(plain, plain)
+    contraction = {}
+    for name, p in (("split", split), ("fp64", plain)):
+        p.set_timing(True)
+        p.timing(reset=True)
+        p.analysis_batch(d_flm, w_sp, s_sp)
+        torch.cuda.synchronize()
+        contraction[name] = p.timing(reset=True).get("lwalk", (0, 0.0))[1] / maps
+        p.set_timing(False)
+    split.check()
+    plain.close()
+    split.close()
+    return {"maps_per_batch": maps, "value": maps / t_split, "unit": "pairs/s",
+            "fp64_same_batch": maps / t_fp64, "speedup_vs_fp64": t_fp64 / t_split,
+            "analysis_contraction_ms_per_map": contraction,
+            "max_w_err": werr, "recon_err": recon,
+            "form": "split analysis (tcgen05 int8 digits, 6 bytes, 28 exact products) + FP64 synthesis",
+            "workload": f"B={B} N={N} alpha={alpha:g} J={J}, {maps} seeded maps per batch, device-resident"}
 
 
 def fft_flops_per_pair(B, N, alpha, J):
@@ -443,6 +518,13 @@ def main():
         except Exception as ex:
             serving = {"error": str(ex)[:300]}
 
+    split = None
+    if args.split_maps > 0:
+        try:
+            split = split_stats(B, N, alpha, J, args.split_maps)
+        except Exception as ex:
+            split = {"error": str(ex)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -463,6 +545,7 @@ def main():
                        "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
                        "recon_err": recon},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
+            "split": split,
             "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
         }
         print(json.dumps(line), flush=True)
