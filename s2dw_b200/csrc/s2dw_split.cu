@@ -400,53 +400,86 @@ __global__ void __launch_bounds__(THREADS) fdig_kernel(FdigArgs a)
 // ---------------------------------------------------------------------------
 // split_kernel
 // ---------------------------------------------------------------------------
+// Thread roles of split_kernel (256 threads, 8 warps):
+//   walker warps 0 .. NWALK-1 (one lane per chain) advance the FP64
+//     recurrence, one 32-row chunk ahead of the cutters;
+//   cutter warps NWALK .. 6 multiply by the factor table and cut digits;
+//   warp 7, lane 0 (the issuer) copies the map digits and issues the MMAs.
+// They hand chunks over through mbarriers: VFULL (chain values written),
+// CUT (digits written, chain values read), done (MMAs finished, tcgen05
+// commit), full (map digits landed, bulk-copy transaction count).  Every wait
+// is bounded; after a timeout every role skips its remaining work but keeps
+// its barrier sequence, so the CTA always reaches the end.
+constexpr int SPLIT_THREADS = 256;
+constexpr int ISSUER_WARP = 7;
+
 template <int NP>
 struct SplitSmem {
     static constexpr int CH = chains(NP);
-    static constexpr int WCH = CH;                      // staged lanes per table row
-    static constexpr int GEN = 0;                       // 2 stages x DIG x A_TILE
-    static constexpr int MAP = GEN + 2 * DIG * A_TILE;  // 2 stages x DIG x B_TILE
-    static constexpr int VB = MAP + 2 * DIG * B_TILE;   // chain values w [chain*33 + li]
-    static constexpr int VB_BYTES = 64 * 33 * 8;
-    // staged tables per buffer (doubles): Ap[KC][WCH], G[KC][NP][WCH], Am[KC], Om[KC]
-    static constexpr int T_AP = 0, T_G = KC * WCH, T_AM = T_G + KC * NP * WCH, T_OM = T_AM + KC;
-    static constexpr int T_DBL = T_OM + KC;
-    static constexpr int TAB = VB + VB_BYTES;
-    static constexpr int PH = TAB + 2 * T_DBL * 8;  // phases [g*16 + n+N-1]
-    static constexpr int EF = PH + 8 * 16 * 16;     // column scale factors 2^(Ef - SHIFT)
-    static constexpr int BAR = EF + COLS * 8;       // full[2], done[2]
-    static constexpr int TM = BAR + 4 * 8;          // TMEM base address
+    static constexpr int NWALK = (CH + 31) / 32;
+    static constexpr int WL = CH < 32 ? CH : 32;             // chains per walker warp
+    static constexpr int NCUT_W = ISSUER_WARP - NWALK;        // cutter warps
+    static constexpr int GEN = 0;                             // 2 stages x DIG x A_TILE
+    static constexpr int MAP = GEN + 2 * DIG * A_TILE;        // 2 stages x DIG x B_TILE
+    static constexpr int VB = MAP + 2 * DIG * B_TILE;         // 2 x [64 chains][33]
+    static constexpr int VB_ONE = 64 * 33;                    // doubles per buffer
+    // walker tables, per walker warp and buffer (doubles): Ap[KC][WL], Am[KC], Om[KC]
+    static constexpr int WT = VB + 2 * VB_ONE * 8;
+    static constexpr int WT_AP = 0, WT_AM = KC * WL, WT_OM = WT_AM + KC, WT_DBL = WT_OM + KC;
+    // factor tables of the cutters, per buffer (doubles): G[KC][NP][CH]
+    static constexpr int GT = WT + NWALK * 2 * WT_DBL * 8;
+    static constexpr int GT_DBL = KC * NP * CH;
+    static constexpr int PH = GT + 2 * GT_DBL * 8;            // phases [g*16 + n+N-1]
+    static constexpr int EF = PH + 8 * 16 * 16;               // column factors 2^(Ef - SHIFT)
+    static constexpr int BAR = EF + COLS * 8;                 // VFULL[2], CUT[2], full[2], done[2]
+    static constexpr int TM = BAR + 8 * 8;
     static constexpr int ABORT = TM + 8;
-    static constexpr int BYTES = ABORT + 8 + 1024;  // + alignment slack
-    static_assert(ROWS * 33 * 8 <= 2 * DIG * A_TILE + 2 * DIG * B_TILE, "epilogue tile fits the operand buffers");
+    static constexpr int BYTES = ABORT + 8 + 1024;            // + alignment slack
+    static constexpr int TS_LD = COLS + 1;                    // epilogue tile row stride
+    static_assert(ROWS * TS_LD * 8 <= WT, "epilogue tile fits the operand and value buffers");
     static_assert(LEV * COLS <= TMEM_COLS, "level accumulators fit TMEM");
+    static_assert(NCUT_W * 32 >= 128, "one cutting item per cutter thread");
 };
 
-// Thread roles: warps 0 (and 1 when CH = 64) walk the chains; thread ISSUER
-// (warp 3, never a walker) issues the MMAs of the previous chunk while the
-// walkers advance, so the walk, the MMA issue and the tensor cores overlap;
-// all 128 threads stage tables, cut digits and run the epilogue.
-constexpr int ISSUER = 96;
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 
 template <int NP>
-__global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
 {
     using S = SplitSmem<NP>;
-    constexpr int CH = S::CH;
+    constexpr int CH = S::CH, NWALK = S::NWALK, WL = S::WL;
     constexpr int PAIRS = CH * NP;  // <= 64
-    constexpr int NWALK = (CH + 31) / 32;
+    constexpr int NCT = S::NCUT_W * 32;
     extern __shared__ unsigned char smraw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    double *vbuf = reinterpret_cast<double *>(sm + S::VB);
     double2 *sPh = reinterpret_cast<double2 *>(sm + S::PH);
     double *sFc = reinterpret_cast<double *>(sm + S::EF);
     uint32_t *sTm = reinterpret_cast<uint32_t *>(sm + S::TM);
     volatile int *sAbort = reinterpret_cast<volatile int *>(sm + S::ABORT);
     const uint32_t bar0 = smem_u32(sm + S::BAR);
-    auto full = [&](int s) { return bar0 + 8 * s; };
-    auto done = [&](int s) { return bar0 + 16 + 8 * s; };
+    auto vfull = [&](int b) { return bar0 + 8 * b; };
+    auto cutb = [&](int b) { return bar0 + 16 + 8 * b; };
+    auto full = [&](int b) { return bar0 + 32 + 8 * b; };
+    auto done = [&](int b) { return bar0 + 48 + 8 * b; };
+    // bounded wait that returns at once after an abort
+    auto wait = [&](uint32_t bar, uint32_t parity) -> bool {
+        if (*sAbort) return false;
+        if (mbar_try(bar, parity)) return true;
+        const unsigned long long t0 = gtimer();
+        while (true) {
+            if (mbar_try(bar, parity)) return true;
+            if (*sAbort || gtimer() - t0 > WAIT_NS) {
+                *sAbort = 1;
+                return false;
+            }
+        }
+    };
 
-    const int t = threadIdx.x, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int2 tile = a.tiles[blockIdx.x];
     const int m = tile.x, p0 = tile.y * CH;
     const int bl = a.bl, blo = a.blo, N = a.N;
@@ -455,10 +488,16 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
     const int cw0 = lw / KC, c_last = (bl - 1) / KC;
     const int c_start = lk / KC;
     const bool has_mma = lk < bl;
+    const int nout = has_mma ? c_last - c_start + 1 : 0;
 
-    // ---- setup: barriers, TMEM, phases, column scales
+    // ---- setup
     if (t == 0) {
-        for (int i = 0; i < 4; i++) mbar_init(bar0 + 8 * i, 1);
+        for (int i = 0; i < 2; i++) {
+            mbar_init(vfull(i), NWALK);
+            mbar_init(cutb(i), S::NCUT_W);
+            mbar_init(full(i), 1);
+            mbar_init(done(i), 1);
+        }
         mbar_fence_init();
         *sAbort = 0;
     }
@@ -466,7 +505,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
         tmem_alloc(smem_u32(sTm), TMEM_COLS);
         tmem_relinquish();
     }
-    for (int i = t; i < N * 16; i += THREADS) sPh[i] = a.ph[i];
+    for (int i = t; i < N * 16; i += SPLIT_THREADS) sPh[i] = a.ph[i];
     if (t < COLS) {
         const int Ef = a.fexp[(size_t)m * COLS + t];
         sFc[t] = Ef > E_MIN ? pow2i(Ef - SHIFT) : 0.0;
@@ -476,156 +515,120 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
     tc_fence_after();
     const uint32_t tmem = *sTm;
 
-    // per-thread digit row pair (also the epilogue row t)
-    const int pair = t >> 1, kh = t & 1;
-    const int pch = pair / NP, pq = pair % NP, pmp = p0 + pch;
-    const bool prow = pair < PAIRS && pmp < bl;
-    const int Ed = prow ? (int)a.dexp[((size_t)m * bl + pmp) * NP + pq] : E_ZERO;
-    const double dfac = digit_factor(Ed);
-    const double rowf = Ed > E_MIN ? pow2i(Ed) : 0.0;
-
-    // walker lanes
-    const bool walker = t < CH;
-    const int wmp = p0 + t;
-    Chain ch;
-    if (warp < NWALK) ch = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
-
-    auto stage_of = [&](int c) { return (c - c_start) & 1; };
-    auto use_of = [&](int c) { return (uint32_t)(((c - c_start) >> 1) & 1); };
-    // map-operand bulk copy of chunk c into its stage (ISSUER or setup)
-    auto issue_map_copy = [&](int c) {
-        const int st = stage_of(c);
-        mbar_expect_tx(full(st), DIG * B_TILE);
-        bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
-                 a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
-    };
-    if (t == 0 && has_mma) issue_map_copy(c_start);
-
-    // MMAs of chunk c (ISSUER): after the MMAs of c-1 finished (their stage
-    // is the one chunk c+1 reuses), start the map copy of c+1, wait for the
-    // map digits of c, issue the digit products of levels < LEV, commit.
-    const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
-                   idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
-    bool first_lev[LEV];
-#pragma unroll
-    for (int i = 0; i < LEV; i++) first_lev[i] = true;
-    auto issue_mmas = [&](int c) -> bool {
-        const int gs = stage_of(c);
-        if (c > c_start && !mbar_wait(done(gs ^ 1), use_of(c - 1), WAIT_NS)) return false;
-        if (c + 1 <= c_last) issue_map_copy(c + 1);
-        if (!mbar_wait(full(gs), use_of(c), WAIT_NS)) return false;
-        tc_fence_after();
-        const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
-        const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
-#pragma unroll
-        for (int i = 0; i < DIG; i++)
-#pragma unroll
-            for (int j = 0; j < DIG; j++) {
-                const int lev = 2 * (DIG - 1) - i - j;
-                if (lev >= LEV) continue;
-                const uint32_t id = (i == DIG - 1) ? (j == DIG - 1 ? idesc_ss : idesc_su)
-                                                   : (j == DIG - 1 ? idesc_us : idesc_uu);
-                mma_i8(tmem + lev * COLS, da0 + (uint64_t)((i * A_TILE) >> 4), db0 + (uint64_t)((j * B_TILE) >> 4),
-                       id, first_lev[lev] ? 0u : 1u);
-                first_lev[lev] = false;
+    if (warp < NWALK) {
+        // ================= walker =================
+        const int ch = warp * 32 + lane;  // chain of this lane
+        const bool walker = lane < WL && ch < CH;
+        const int wmp = p0 + ch;
+        Chain cn = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
+        double *WT = reinterpret_cast<double *>(sm + S::WT) + warp * 2 * S::WT_DBL;
+        auto stage = [&](int c, int b) {
+            double *T = WT + b * S::WT_DBL;
+            const int lb = c * KC;
+            constexpr int V = WL / 2;
+            for (int i = lane; i < KC * V; i += 32) {
+                const int li = i / V, x = 2 * (i % V), l = lb + li, col = p0 + warp * 32 + x;
+                double *d = T + S::WT_AP + li * WL + x;
+                if (l < bl && col < a.Bp) cp_async16(d, a.Acoef + (size_t)l * a.Bp + col);
+                else { d[0] = 0.0; d[1] = 0.0; }
             }
-        mma_commit(done(gs));
-        return true;
-    };
-
-    // staged tables for chunk c -> buffer b
-    auto stage_tables = [&](int c, int b) {
-        double *T = reinterpret_cast<double *>(sm + S::TAB) + b * S::T_DBL;
-        const int lb = c * KC;
-        constexpr int V = S::WCH / 2;  // 16-byte pieces per row
-        for (int i = t; i < KC * V; i += THREADS) {
-            const int li = i / V, x = 2 * (i % V), l = lb + li;
-            double *d = T + S::T_AP + li * S::WCH + x;
-            if (l < bl && p0 + x < a.Bp) cp_async16(d, a.Acoef + (size_t)l * a.Bp + p0 + x);
-            else { d[0] = 0.0; d[1] = 0.0; }
-        }
-        for (int i = t; i < KC * NP * V; i += THREADS) {
-            const int li = i / (NP * V), r = i % (NP * V), q = r / V, x = 2 * (r % V), l = lb + li;
-            double *d = T + S::T_G + (li * NP + q) * S::WCH + x;
-            if (l < bl && l > blo && p0 + x < a.Gs)
-                cp_async16(d, a.G + ((size_t)(l - blo - 1) * NP + q) * a.Gs + p0 + x);
-            else { d[0] = 0.0; d[1] = 0.0; }
-        }
-        for (int i = t; i < 2 * KC; i += THREADS) {
-            const int li = i % KC, l = lb + li;
-            double *d = T + (i < KC ? S::T_AM : S::T_OM) + li;
-            const double *src = (i < KC ? a.Acoef : a.Om) + (size_t)l * a.Bp + m;
-            if (l < bl) cp_async8(d, src);
-            else *d = 0.0;
-        }
-    };
-
-    int pending = -1;  // chunk whose digits are ready and whose MMAs are not issued
-    if (has_mma) {
-        stage_tables(cw0, 0);
-        cp_commit_all();
-        cp_wait_all();
-        __syncthreads();
-        for (int c = cw0; c <= c_last; c++) {
-            const int tb = (c - cw0) & 1;
-            if (c + 1 <= c_last) stage_tables(c + 1, tb ^ 1);
+            for (int i = lane; i < 2 * KC; i += 32) {
+                const int li = i % KC, l = lb + li;
+                double *d = T + (i < KC ? S::WT_AM : S::WT_OM) + li;
+                if (l < bl) cp_async8(d, (i < KC ? a.Acoef : a.Om) + (size_t)l * a.Bp + m);
+                else *d = 0.0;
+            }
+        };
+        if (has_mma) {
+            stage(cw0, 0);
             cp_commit_all();
-            const double *T = reinterpret_cast<const double *>(sm + S::TAB) + tb * S::T_DBL;
-            const bool out = c >= c_start;
-            if (t == ISSUER && pending >= 0 && !issue_mmas(pending)) *sAbort = 1;
-            // ---- walk: chain values w(l) of this chunk, coefficients read in
-            // blocks of 8 rows so that their loads overlap the recurrence
-            if (warp < NWALK) {
+            for (int c = cw0; c <= c_last; c++) {
+                const int wb = (c - cw0) & 1;
+                if (c + 1 <= c_last) stage(c + 1, wb ^ 1);
+                cp_commit_all();
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+                __syncwarp();
+                const double *T = WT + wb * S::WT_DBL;
+                const int k = c - c_start;
+                const bool out = k >= 0;
+                if (out && k >= 2) wait(cutb(k & 1), ((k - 2) >> 1) & 1);  // cutters done with chunk k-2
                 const int lb = c * KC;
                 const int lo = max(lb, lw) - lb, hi = min(lb + KC, bl) - lb;
-                double *vrow = vbuf + t * 33;
+                double *vrow = reinterpret_cast<double *>(sm + S::VB) + (k & 1) * S::VB_ONE + ch * 33;
                 if (lo == 0 && hi == KC) {
-                    // full chunk: straight-line 32 steps, values kept in
-                    // registers until the walk ends so that no store orders
-                    // the coefficient loads (renormalisation at l = 15, 31 mod 32)
                     double wv[KC];
 #pragma unroll
                     for (int li = 0; li < KC; li++) {
-                        wv[li] = chain_step(ch, lb + li, T[S::T_AM + li], walker ? T[S::T_AP + li * S::WCH + t] : 0.0,
-                                            T[S::T_OM + li]);
-                        if ((li & 15) == 15) chain_renorm(ch);
+                        wv[li] = chain_step(cn, lb + li, T[S::WT_AM + li], walker ? T[S::WT_AP + li * WL + lane] : 0.0,
+                                            T[S::WT_OM + li]);
+                        if ((li & 15) == 15) chain_renorm(cn);
                     }
                     if (out && walker) {
 #pragma unroll
                         for (int li = 0; li < KC; li++) vrow[li] = wv[li];
                     }
-                } else
-                for (int li0 = 0; li0 < KC; li0 += 8) {
-                    double am[8], ap[8], om[8];
-#pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        am[u] = T[S::T_AM + li0 + u];
-                        ap[u] = walker ? T[S::T_AP + (li0 + u) * S::WCH + t] : 0.0;
-                        om[u] = T[S::T_OM + li0 + u];
-                    }
-#pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        const int li = li0 + u, l = lb + li;
+                } else {
+                    for (int li = 0; li < KC; li++) {
+                        const int l = lb + li;
                         double w = 0.0;
                         if (li >= lo && li < hi) {
-                            w = chain_step(ch, l, am[u], ap[u], om[u]);
-                            if ((l & 15) == 15) chain_renorm(ch);
+                            w = chain_step(cn, l, T[S::WT_AM + li], walker ? T[S::WT_AP + li * WL + lane] : 0.0,
+                                           T[S::WT_OM + li]);
+                            if ((l & 15) == 15) chain_renorm(cn);
                         }
                         if (out && walker) vrow[li] = w;
                     }
                 }
+                __syncwarp();
+                if (out && lane == 0) mbar_arrive(vfull(k & 1));
             }
-            __syncthreads();
-            if (out) {
-                // ---- digits of rows 2*pair (+) and 2*pair+1 (-): v = w * G
-                unsigned char *gen = sm + S::GEN + stage_of(c) * DIG * A_TILE;
+            cp_wait_all();
+        }
+    } else if (warp < ISSUER_WARP) {
+        // ================= cutters =================
+        const int ct = t - NWALK * 32;
+        const bool item = ct < 128;
+        const int pair = ct >> 1, kh = ct & 1;
+        const int pch = pair / NP, pq = pair % NP, pmp = p0 + pch;
+        const bool prow = item && pair < PAIRS && pmp < bl;
+        const int Ed = prow ? (int)a.dexp[((size_t)m * bl + pmp) * NP + pq] : E_ZERO;
+        const double dfac = digit_factor(Ed);
+        double *GT = reinterpret_cast<double *>(sm + S::GT);
+        auto stage = [&](int c, int b) {
+            double *T = GT + b * S::GT_DBL;
+            const int lb = c * KC;
+            constexpr int V = CH / 2;
+            for (int i = ct; i < KC * NP * V; i += NCT) {
+                const int li = i / (NP * V), r = i % (NP * V), q = r / V, x = 2 * (r % V), l = lb + li;
+                double *d = T + (li * NP + q) * CH + x;
+                if (l < bl && l > blo && p0 + x < a.Gs)
+                    cp_async16(d, a.G + ((size_t)(l - blo - 1) * NP + q) * a.Gs + p0 + x);
+                else { d[0] = 0.0; d[1] = 0.0; }
+            }
+        };
+        if (nout > 0) {
+            stage(c_start, 0);
+            cp_commit_all();
+        }
+        for (int k = 0; k < nout; k++) {
+            const int c = c_start + k, gb = k & 1;
+            if (k + 1 < nout) stage(c + 1, gb ^ 1);
+            cp_commit_all();
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            named_sync(1, NCT);  // G of chunk k visible to every cutter
+            bool ok = wait(vfull(k & 1), (k >> 1) & 1);
+            if (k >= 2) ok = wait(done(k & 1), ((k - 2) >> 1) & 1) && ok;  // MMAs of chunk k-2 finished
+            if (ok && item) {
+                const double *T = GT + gb * S::GT_DBL;
+                const double *vb = reinterpret_cast<const double *>(sm + S::VB) + (k & 1) * S::VB_ONE;
+                unsigned char *gen = sm + S::GEN + (k & 1) * DIG * A_TILE;
                 const int lb = c * KC;
                 long long X[16];
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const int li = 16 * kh + i, l = lb + li;
                     double v = 0.0;
-                    if (prow && l > blo) v = vbuf[pch * 33 + li] * T[S::T_G + (li * NP + pq) * S::WCH + pch];
+                    if (prow && l > blo) v = vb[pch * 33 + li] * T[(li * NP + pq) * CH + pch];
                     X[i] = to_fixed(v, dfac);
                 }
                 store_digits(gen + tile_off(ROWS, 2 * pair, kh), A_TILE, X);
@@ -633,81 +636,120 @@ __global__ void __launch_bounds__(THREADS, 1) split_kernel(SplitArgs a)
                 for (int i = 1; i < 16; i += 2) X[i] = -X[i];  // (-1)^l, l = 32c + 16kh + i
                 store_digits(gen + tile_off(ROWS, 2 * pair + 1, kh), A_TILE, X);
                 fence_async_smem();
-                pending = c;
             }
-            cp_wait_all();
-            __syncthreads();
-            if (*sAbort) break;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(cutb(k & 1));
+            named_sync(1, NCT);  // every cutter finished with G buffer gb
         }
-        // ---- the last chunk's MMAs, then drain
-        if (t == ISSUER && !*sAbort) {
-            if (!issue_mmas(c_last) || !mbar_wait(done(stage_of(c_last)), use_of(c_last), WAIT_NS)) *sAbort = 1;
+        cp_wait_all();
+    } else if (lane == 0 && nout > 0) {
+        // ================= issuer =================
+        auto map_copy = [&](int c) {
+            const int st = (c - c_start) & 1;
+            mbar_expect_tx(full(st), DIG * B_TILE);
+            bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
+                     a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
+        };
+        const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
+                       idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
+        bool first_lev[LEV];
+#pragma unroll
+        for (int i = 0; i < LEV; i++) first_lev[i] = true;
+        map_copy(c_start);
+        for (int k = 0; k < nout; k++) {
+            const int gs = k & 1, c = c_start + k;
+            if (!wait(cutb(gs), (k >> 1) & 1)) continue;
+            if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
+            if (k + 1 < nout) map_copy(c + 1);
+            if (!wait(full(gs), (k >> 1) & 1)) continue;
+            tc_fence_after();
+            const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
+            const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
+#pragma unroll
+            for (int i = 0; i < DIG; i++)
+#pragma unroll
+                for (int j = 0; j < DIG; j++) {
+                    const int lev = 2 * (DIG - 1) - i - j;
+                    if (lev >= LEV) continue;
+                    const uint32_t id = (i == DIG - 1) ? (j == DIG - 1 ? idesc_ss : idesc_su)
+                                                       : (j == DIG - 1 ? idesc_us : idesc_uu);
+                    mma_i8(tmem + lev * COLS, da0 + (uint64_t)((i * A_TILE) >> 4),
+                           db0 + (uint64_t)((j * B_TILE) >> 4), id, first_lev[lev] ? 0u : 1u);
+                    first_lev[lev] = false;
+                }
+            mma_commit(done(gs));
         }
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
+        wait(done((nout - 1) & 1), ((nout - 1) >> 1) & 1);
     }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
 
     const bool abort = *sAbort != 0;
     if (abort && t == 0) atomicExch(a.err, 1);
 
-    // ---- epilogue: two halves of 32 columns (16 maps)
-    double *Ts = reinterpret_cast<double *>(sm + S::GEN);  // [row * 33 + col]
-    const int ev = (N % 2 == 0) ? 1 : 0;
-    for (int h = 0; h < 2; h++) {
+    // ---- epilogue: warp w reads TMEM lanes 32*(w&3).. (rows) and columns
+    // [32*(w>>2), +32) (maps 16*(w>>2) .. +16)
+    double *Ts = reinterpret_cast<double *>(sm + S::GEN);  // [row * TS_LD + col]
+    {
+        const int row = 32 * (warp & 3) + lane, half = warp >> 2;
+        const int rp = row >> 1, rch = rp / NP, rq = rp % NP, rmp = p0 + rch;
+        const int Er = (rp < PAIRS && rmp < bl) ? (int)a.dexp[((size_t)m * bl + rmp) * NP + rq] : E_ZERO;
+        const double rowf = Er > E_MIN ? pow2i(Er) : 0.0;
         for (int blk = 0; blk < 2; blk++) {
-            const int col0 = 32 * h + 16 * blk;
+            const int col0 = 32 * half + 16 * blk;
             double acc[16];
 #pragma unroll
             for (int i = 0; i < 16; i++) acc[i] = 0.0;
-            if (has_mma && !abort) {
+            if (nout > 0 && !abort) {
 #pragma unroll
                 for (int lev = 0; lev < LEV; lev++) {
                     int32_t r[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + lev * COLS + col0, r);
+                    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + lev * COLS + col0, r);
                     const double wgt = pow2i(-8 * lev);
 #pragma unroll
                     for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 16; i++) Ts[t * 33 + 16 * blk + i] = (acc[i] * rowf) * sFc[col0 + i];
+            for (int i = 0; i < 16; i++) Ts[row * S::TS_LD + col0 + i] = (acc[i] * rowf) * sFc[col0 + i];
         }
-        __syncthreads();
-        // (chain, map) items of this half
-        constexpr int ITEMS = CH * 16;
-        for (int it = t; it < ITEMS; it += THREADS) {
-            const int c = it % CH, kk = it / CH, k = 16 * h + kk, mp = p0 + c;
-            if (mp >= bl || k >= a.nmaps) continue;
-            double2 Tp[NP], Tm[NP];
+    }
+    __syncthreads();
+    // (chain, map) items
+    const int ev = (N % 2 == 0) ? 1 : 0;
+    constexpr int ITEMS = CH * MAPS;
+    for (int it = t; it < ITEMS; it += SPLIT_THREADS) {
+        const int c = it % CH, k = it / CH, mp = p0 + c;
+        if (mp >= bl || k >= a.nmaps) continue;
+        double2 Tp[NP], Tm[NP];
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            const int n = a.nq[q], pr = c * NP + q;
+            const double2 sum = make_double2(Ts[(2 * pr) * S::TS_LD + 2 * k], Ts[(2 * pr) * S::TS_LD + 2 * k + 1]);
+            const double2 dif =
+                make_double2(Ts[(2 * pr + 1) * S::TS_LD + 2 * k], Ts[(2 * pr + 1) * S::TS_LD + 2 * k + 1]);
+            if (n == 0) {
+                Tp[q] = c_ipow(sum, -m);
+                Tm[q] = make_double2(0.0, 0.0);
+            } else {
+                Tp[q] = c_ipow(sum, n - m - ev);
+                double2 x = c_ipow(dif, -n - m + ev);
+                if ((mp + n) & 1) x = make_double2(-x.x, -x.y);
+                Tm[q] = x;
+            }
+        }
+        double2 *out = a.Tg + (size_t)k * N * bl * bl;
+        for (int g = 0; g < N; g++) {
+            double2 y = make_double2(0.0, 0.0);
 #pragma unroll
             for (int q = 0; q < NP; q++) {
-                const int n = a.nq[q], pr = c * NP + q;
-                const double2 sum = make_double2(Ts[(2 * pr) * 33 + 2 * kk], Ts[(2 * pr) * 33 + 2 * kk + 1]);
-                const double2 dif = make_double2(Ts[(2 * pr + 1) * 33 + 2 * kk], Ts[(2 * pr + 1) * 33 + 2 * kk + 1]);
-                if (n == 0) {
-                    Tp[q] = c_ipow(sum, -m);
-                    Tm[q] = make_double2(0.0, 0.0);
-                } else {
-                    Tp[q] = c_ipow(sum, n - m - ev);
-                    double2 x = c_ipow(dif, -n - m + ev);
-                    if ((mp + n) & 1) x = make_double2(-x.x, -x.y);
-                    Tm[q] = x;
-                }
+                const int n = a.nq[q];
+                y = c_add(y, c_mul(Tp[q], sPh[g * 16 + n + N - 1]));
+                if (n != 0) y = c_add(y, c_mul(Tm[q], sPh[g * 16 - n + N - 1]));
             }
-            double2 *out = a.Tg + (size_t)k * N * bl * bl;
-            for (int g = 0; g < N; g++) {
-                double2 y = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int q = 0; q < NP; q++) {
-                    const int n = a.nq[q];
-                    y = c_add(y, c_mul(Tp[q], sPh[g * 16 + n + N - 1]));
-                    if (n != 0) y = c_add(y, c_mul(Tm[q], sPh[g * 16 - n + N - 1]));
-                }
-                out[((size_t)g * bl + m) * bl + mp] = y;
-            }
+            out[((size_t)g * bl + m) * bl + mp] = y;
         }
-        __syncthreads();
     }
     tc_fence_before();
     __syncthreads();
@@ -751,7 +793,7 @@ static int launch_split_t(const SplitArgs &a, cudaStream_t s)
         S2DW_CUDA_TRY(cudaFuncSetAttribute(split::split_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr = true;
     }
-    split::split_kernel<NP><<<a.ntiles, split::THREADS, bytes, s>>>(a);
+    split::split_kernel<NP><<<a.ntiles, split::SPLIT_THREADS, bytes, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
