@@ -221,6 +221,41 @@ struct FdigArgs {
     uint8_t *fdig;
 };
 
+// Synthesis counterpart: for one m, rows are 128 chains l (m'-walk of
+// d^l_{m'm}), K runs over (m', q) with MC m' and NPQ (power of two >= NP)
+// values of q per 32-byte K step, columns are (map, re/im).
+struct SplitSynArgs {
+    int B, Bp, N, NP, bl, blo;
+    int nch, nmaps;            // 32-row K chunks per m (MC m' each), maps (<= 32)
+    const double *Bcoef;       // [l*Bp + m']
+    const double *Em;          // [l*B + m]
+    const int32_t *Ee;
+    const double *G;           // as MwalkArgs::G
+    int Gs;
+    int16_t *sexp;             // [m*bl + l] exponent of max over (m', q) of |v|
+    const int32_t *vexp;       // [m*64 + col]
+    const uint8_t *vdig;       // [(m*nch + chunk)*6 + digit][2048] map digits
+    double2 *part;             // map k: part + k*pstride, [(l-blo-1)*bl + m]
+    long long pstride;
+    const int2 *tiles;         // (m, 128-row l tile)
+    int ntiles;
+    int *err;
+};
+
+struct VdigArgs {
+    int bl, NP, nch, nmaps, Vs;
+    const double2 *V2f;        // map k: V2f + k*vstride, [(q*bl + m)*Vs + m']
+    long long vstride;
+    int32_t *vexp;
+    uint8_t *vdig;
+};
+
+int split_syn_mc(int NP);       // m' per K chunk
+long long split_vdig_bytes(int bl, int nch);
+int launch_split_syn_dexp(const SplitSynArgs &a, cudaStream_t s);
+int launch_split_vdig(const VdigArgs &a, cudaStream_t s);
+int launch_split_syn(const SplitSynArgs &a, cudaStream_t s);
+
 int split_chains(int NP);       // m' per CTA
 int split_maps_per_pass();      // maps per CTA
 long long split_fdig_bytes(int bl, int nch);

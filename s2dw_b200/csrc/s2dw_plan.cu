@@ -71,6 +71,10 @@ struct s2dwc_plan {
         int c0 = 0, nch = 0, ntiles = 0;
         int2 *tiles = nullptr;
         long long dexp_off = 0;
+        // synthesis
+        int snch = 0, sntiles = 0;
+        int2 *stiles = nullptr;
+        long long sexp_off = 0;
     };
     std::vector<SplitScale> sp;
     bool sp_alloc = false, sp_dexp_valid = false;
@@ -78,6 +82,11 @@ struct s2dwc_plan {
     int32_t *sp_fexp = nullptr;
     uint8_t *sp_fdig = nullptr;
     double2 *sp_Tg = nullptr, *sp_Tb = nullptr, *sp_ph = nullptr;
+    int16_t *sp_sexp = nullptr;
+    int32_t *sp_vexp = nullptr;
+    uint8_t *sp_vdig = nullptr;
+    double2 *sp_V2f = nullptr, *sp_part = nullptr;
+    long long sp_vstride = 0, sp_pstride = 0;
     int *sp_err = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
@@ -633,6 +642,34 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             S.ntiles = (int)tl.size();
             if ((st = dev_upload(p, &S.tiles, tl))) return st;
         }
+        // synthesis: (m, 128-row l tile) tiles, m-major so that the tiles of one m
+        // share the map digits in L2
+        long long ns = 0, vdig = 0;
+        const int MC = split_syn_mc(NP);
+        for (int j = 0; j <= p->J; j++) {
+            auto &S = p->sp[j];
+            const int bl = p->bl[j], blo = p->blo[j], nl = bl - blo - 1;
+            S.snch = (bl + MC - 1) / MC;
+            S.sexp_off = ns;
+            ns += (long long)bl * bl;
+            vdig = std::max(vdig, split_vdig_bytes(bl, S.snch));
+            std::vector<int2> tl;
+            for (int m = 0; m < bl; m++)
+                for (int lt = 0; lt * 128 < nl; lt++) {
+                    const int lbase = blo + 1 + lt * 128;
+                    if (m <= std::min(lbase + 127, bl - 1)) tl.push_back(make_int2(m, lt));
+                }
+            S.sntiles = (int)tl.size();
+            if (tl.empty()) tl.push_back(make_int2(0, 0));
+            if ((st = dev_upload(p, &S.stiles, tl))) return st;
+        }
+        p->sp_vstride = (long long)p->NP * blmax * ((blmax + 7) / 8 * 8);
+        p->sp_pstride = std::max(1LL, p->offP.back() + (long long)std::max(0, p->bl[p->J] - p->blo[p->J] - 1) * p->bl[p->J]);
+        if ((st = dev_alloc(p, &p->sp_sexp, (size_t)ns)) || (st = dev_alloc(p, &p->sp_vexp, (size_t)blmax * 64)) ||
+            (st = dev_alloc(p, &p->sp_vdig, (size_t)vdig)) ||
+            (st = dev_alloc(p, &p->sp_V2f, (size_t)MAPS * p->sp_vstride)) ||
+            (st = dev_alloc(p, &p->sp_part, (size_t)MAPS * p->sp_pstride)))
+            return st;
         const long long b2 = (long long)blmax * blmax;
         if ((st = dev_alloc(p, &p->sp_dexp, (size_t)nd)) || (st = dev_alloc(p, &p->sp_fexp, (size_t)blmax * 64)) ||
             (st = dev_alloc(p, &p->sp_fdig, (size_t)fdig)) ||
@@ -670,6 +707,22 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             a.tiles = p->sp[j].tiles;
             a.ntiles = p->sp[j].ntiles;
             if ((st = launch_split_dexp(a, s))) return st;
+            SplitSynArgs b{};
+            b.B = p->B;
+            b.Bp = p->Bp;
+            b.N = p->N;
+            b.NP = NP;
+            b.bl = p->bl[j];
+            b.blo = p->blo[j];
+            b.Bcoef = p->Bcoef;
+            b.Em = p->Em;
+            b.Ee = p->Ee;
+            b.G = p->Gsyn + p->gs_off[j];
+            b.Gs = p->gs_stride[j];
+            b.sexp = p->sp_sexp + p->sp[j].sexp_off;
+            b.tiles = p->sp[j].stiles;
+            b.ntiles = p->sp[j].sntiles;
+            if ((st = launch_split_syn_dexp(b, s))) return st;
         }
         p->sp_dexp_valid = true;
     }
@@ -769,6 +822,117 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             if ((st = launch_scoeff_copy(d_scoeff ? d_scoeff + (g0 + k) * bs2 : nullptr, d_flm + (g0 + k) * B2, p->B,
                                          p->bl_scoeff, s)))
                 return st;
+        }
+    }
+    return S2DWC_OK;
+}
+
+// Split-form synthesis of `nmaps` maps (layouts as run_analysis_split): per
+// group of up to 32 maps and per scale, the alpha and beta transforms map by
+// map into a batch of V tables, their digits, the tensor-core contraction
+// into per-map partial rows; then the scale sum of each map.
+int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *d_wav, const double2 *d_scoeff,
+                        cudaStream_t s)
+{
+    int st;
+    if ((st = split_prepare(p, s))) return st;
+    const int MAPS = split_maps_per_pass();
+    const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
+    const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
+    for (int g0 = 0; g0 < nmaps; g0 += MAPS) {
+        const int nk = std::min(MAPS, nmaps - g0);
+        for (int j = 0; j <= p->J; j++) {
+            const int bl = p->bl[j];
+            const auto &S = p->sp[j];
+            for (int k = 0; k < nk; k++) {
+                CztArgs ca{};
+                ca.mode = CZT_SYN_ALPHA;
+                ca.bl = bl;
+                ca.N = p->N;
+                ca.NP = p->NP;
+                std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
+                ca.rows = p->N * bl;
+                ca.czt = p->czt[j][CZT_SYN_ALPHA];
+                ca.tw = p->tw.at(ca.czt.M);
+                ca.in_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
+                ca.out_c = p->sp_Tb;
+                ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
+                {
+                    KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, s);
+                    if ((st = launch_czt(ca, s))) return st;
+                }
+                ca.mode = p->syn_beta_mode[j];
+                ca.rows = p->NP * bl;
+                ca.czt = p->czt[j][ca.mode];
+                ca.tw = p->tw.at(ca.czt.M);
+                ca.in_c = p->sp_Tb;
+                ca.in_r = nullptr;
+                ca.out_c = p->sp_V2f + k * p->sp_vstride;
+                ca.out_stride = p->gs_stride[j];
+                ca.wq = p->wq[j];
+                {
+                    KernelTimer kt(p, S2DWC_KIND_SYN_BETA, s);
+                    if ((st = launch_czt(ca, s))) return st;
+                }
+            }
+            if (bl - p->blo[j] - 1 <= 0) continue;
+            VdigArgs va{};
+            va.bl = bl;
+            va.NP = p->NP;
+            va.nch = S.snch;
+            va.nmaps = nk;
+            va.Vs = p->gs_stride[j];
+            va.V2f = p->sp_V2f;
+            va.vstride = p->sp_vstride;
+            va.vexp = p->sp_vexp;
+            va.vdig = p->sp_vdig;
+            {
+                KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+                if ((st = launch_split_vdig(va, s))) return st;
+            }
+            SplitSynArgs b{};
+            b.B = p->B;
+            b.Bp = p->Bp;
+            b.N = p->N;
+            b.NP = p->NP;
+            b.bl = bl;
+            b.blo = p->blo[j];
+            b.nch = S.snch;
+            b.nmaps = nk;
+            b.Bcoef = p->Bcoef;
+            b.Em = p->Em;
+            b.Ee = p->Ee;
+            b.G = p->Gsyn + p->gs_off[j];
+            b.Gs = p->gs_stride[j];
+            b.sexp = p->sp_sexp + S.sexp_off;
+            b.vexp = p->sp_vexp;
+            b.vdig = p->sp_vdig;
+            b.part = p->sp_part + p->offP[j];
+            b.pstride = p->sp_pstride;
+            b.tiles = S.stiles;
+            b.ntiles = S.sntiles;
+            b.err = p->sp_err;
+            {
+                KernelTimer kt(p, S2DWC_KIND_MWALK, s);
+                if ((st = launch_split_syn(b, s))) return st;
+            }
+        }
+        for (int k = 0; k < nk; k++) {
+            CombineArgs cb{};
+            cb.B = p->B;
+            cb.J = p->J;
+            cb.bs = p->bl_scoeff;
+            for (int j = 0; j <= p->J; j++) {
+                cb.bl[j] = p->bl[j];
+                cb.blo[j] = p->blo[j];
+                cb.off[j] = p->offP[j];
+            }
+            cb.parts = p->sp_part + k * p->sp_pstride;
+            cb.scoeff = d_scoeff ? d_scoeff + (g0 + k) * bs2 : nullptr;
+            cb.Phi2 = p->Phi2;
+            cb.flm = d_flm + (g0 + k) * B2;
+            KernelTimer kt(p, S2DWC_KIND_OTHER, s);
+            if ((st = launch_combine(cb, s))) return st;
         }
     }
     return S2DWC_OK;
@@ -1033,6 +1197,9 @@ int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const do
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: nmaps=%d", nmaps);
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis_batch: tables not set");
     DeviceGuard dg(p->device);
+    if (p->form == S2DWC_FORM_SPLIT)
+        return run_synthesis_split(p, nmaps, reinterpret_cast<double2 *>(d_flm), d_wav,
+                                   reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
     const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
     const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
     for (int k = 0; k < nmaps; k++) {
@@ -1061,6 +1228,9 @@ int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, cons
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis: null pointer");
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis: tables not set");
     DeviceGuard dg(p->device);
+    if (p->form == S2DWC_FORM_SPLIT)
+        return run_synthesis_split(p, 1, reinterpret_cast<double2 *>(d_flm), d_wav,
+                                   reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
     return run_synthesis(p, reinterpret_cast<double2 *>(d_flm), d_wav,
                          reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
 }

@@ -756,6 +756,347 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
     if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
 }
 
+// ===========================================================================
+// Synthesis: the contraction of s2dw_core_mod.f90:1200-1253 for a batch,
+//
+//   part^k(l, m) = i^m sum_{m' <= l} sum_q v(m'; l, m, q) V^k(q, m, m'),
+//   v = d^l_{m'm}(pi/2) d^l_{m'n_q}(pi/2) c_j(l, n_q),
+//
+// a GEMM per m with rows l (chains of the m'-recurrence, 128 per CTA), K over
+// (m', q) and columns (map, re/im).  Same digits, levels and TMEM layout as
+// the analysis; the walker warps cut their own rows (no +-n rows here).
+// ===========================================================================
+__host__ __device__ constexpr int syn_npq(int NP) { return NP == 1 ? 1 : (NP == 2 ? 2 : 4); }
+__host__ __device__ constexpr int syn_mc(int NP) { return KC / syn_npq(NP); }
+constexpr int SYN_ROWS = 128;
+
+// m'-walk of chain (l, m): the recurrence of mwalk_kernel, e_{m'-1} =
+// m b(l,m') e_{m'} - e_{m'+1}, started at m' = l.
+__device__ __forceinline__ Chain syn_chain_init(const int32_t *Ee, const double *Em, int B, int l, int m, bool valid)
+{
+    Chain c;
+    c.e = 0.0;
+    c.ep = 0.0;
+    c.st = 0.0;
+    c.l0 = valid ? l : INT_MAX;
+    int maxe = valid ? (int)Ee[(size_t)l * B + m] : INT_MIN;
+    maxe = wmax_i(maxe);
+    c.Kw = (maxe != INT_MIN && maxe < S2DW_SCALE_EXP) ? -maxe : 0;
+    c.sc = pow2_or_zero(-c.Kw);
+    if (valid) {
+        const double v = ldexp(Em[(size_t)l * B + m], (int)Ee[(size_t)l * B + m] + c.Kw);
+        c.st = ((l - m) & 1) ? -v : v;
+    }
+    return c;
+}
+// value at m' (true scale), then one step down; p = m b(l, m')
+__device__ __forceinline__ double syn_chain_step(Chain &c, int mp, double p)
+{
+    if (mp == c.l0) c.e = c.st;
+    const double w = c.e * c.sc;
+    const double en = fma(p, c.e, -c.ep);
+    c.ep = c.e;
+    c.e = en;
+    return w;
+}
+
+// sexp: exponent of max over (m', q) of |v| per chain; one CTA per tile.
+template <int NP>
+__global__ void __launch_bounds__(SYN_ROWS) syn_dexp_kernel(SplitSynArgs a)
+{
+    const int2 tile = a.tiles[blockIdx.x];
+    const int m = tile.x, lbase = a.blo + 1 + tile.y * SYN_ROWS;
+    const int l = lbase + threadIdx.x;
+    const int MH = min(lbase + SYN_ROWS - 1, a.bl - 1);
+    const bool valid = l < a.bl && m <= l;
+    Chain c = syn_chain_init(a.Ee, a.Em, a.B, l, m, valid);
+    const int lc = min(l, a.bl - 1);
+    const double mm = (double)m;
+    double mx = 0.0;
+#pragma unroll 4
+    for (int mp = MH; mp >= 0; mp--) {
+        const double w = syn_chain_step(c, mp, mm * a.Bcoef[(size_t)lc * a.Bp + mp]);
+        if (valid && mp <= l) {
+#pragma unroll
+            for (int q = 0; q < NP; q++)
+                mx = fmax(mx, fabs(w * a.G[((size_t)(l - a.blo - 1) * NP + q) * a.Gs + mp]));
+        }
+        if ((mp & 15) == 0) chain_renorm(c);
+    }
+    if (valid) a.sexp[(size_t)m * a.bl + l] = (int16_t)(mx > 0.0 ? ilogb(mx) + 1 : E_ZERO);
+}
+
+// Map digits of the synthesis: column col = 2k + (re, im) of V^k(q, m, m');
+// K index within chunk ci: kk = (m' - MC ci) * NPQ + q.  One CTA per m.
+template <int NP>
+__global__ void __launch_bounds__(THREADS) vdig_kernel(VdigArgs a)
+{
+    constexpr int NPQ = syn_npq(NP), MC = syn_mc(NP);
+    __shared__ int sE[COLS];
+    const int m = blockIdx.x, t = threadIdx.x;
+    const int col = t >> 1, half = t & 1, k = col >> 1, comp = col & 1;
+    const double *V = reinterpret_cast<const double *>(a.V2f + (size_t)k * a.vstride) + comp;
+    double mx = 0.0;
+    if (k < a.nmaps)
+        for (int q = 0; q < NP; q++)
+            for (int mp = half; mp < a.bl; mp += 2)
+                mx = fmax(mx, fabs(V[2 * (((size_t)q * a.bl + m) * a.Vs + mp)]));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    const int E = mx > 0.0 ? ilogb(mx) + 1 : E_ZERO;
+    if (half == 0) {
+        sE[col] = E;
+        a.vexp[(size_t)m * COLS + col] = E;
+    }
+    __syncthreads();
+    const double factor = digit_factor(sE[col]);
+    const int kh = half;
+    for (int ci = 0; ci < a.nch; ci++) {
+        long long X[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int kk = 16 * kh + i, q = kk % NPQ, mp = ci * MC + kk / NPQ;
+            const double v = (k < a.nmaps && q < NP && mp < a.bl) ? V[2 * (((size_t)q * a.bl + m) * a.Vs + mp)] : 0.0;
+            X[i] = to_fixed(v, factor);
+        }
+        unsigned char *dst = a.vdig + ((size_t)m * a.nch + ci) * DIG * B_TILE + tile_off(COLS, col, kh);
+        store_digits(dst, B_TILE, X);
+    }
+}
+
+template <int NP>
+struct SynSmem {
+    static constexpr int NPQ = syn_npq(NP), MC = syn_mc(NP);
+    static constexpr int RS = MC + 2;                         // padded table row (16-byte aligned)
+    static constexpr int GEN = 0;                             // 2 stages x DIG x A_TILE
+    static constexpr int MAP = GEN + 2 * DIG * A_TILE;        // 2 stages x DIG x B_TILE
+    // lane-private staged rows per buffer (doubles): b[128][RS], G[128][NP][RS]
+    static constexpr int TB = MAP + 2 * DIG * B_TILE;
+    static constexpr int T_B = 0, T_G = SYN_ROWS * RS, T_DBL = T_G + SYN_ROWS * NP * RS;
+    static constexpr int EF = TB + 2 * T_DBL * 8;
+    static constexpr int BAR = EF + COLS * 8;                 // gfull[2], full[2], done[2]
+    static constexpr int TM = BAR + 6 * 8;
+    static constexpr int ABORT = TM + 8;
+    static constexpr int BYTES = ABORT + 8 + 1024;
+    static_assert(LEV * COLS <= TMEM_COLS, "level accumulators fit TMEM");
+    static_assert(BYTES <= 227 * 1024, "shared memory");
+};
+
+// Roles (256 threads): warps 0-3 walk the 128 chains and cut their own rows;
+// warp 7 lane 0 issues the map copies and MMAs; all warps run the epilogue.
+template <int NP>
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArgs a)
+{
+    using S = SynSmem<NP>;
+    constexpr int NPQ = S::NPQ, MC = S::MC, RS = S::RS;
+    extern __shared__ unsigned char smraw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    double *sFc = reinterpret_cast<double *>(sm + S::EF);
+    uint32_t *sTm = reinterpret_cast<uint32_t *>(sm + S::TM);
+    volatile int *sAbort = reinterpret_cast<volatile int *>(sm + S::ABORT);
+    const uint32_t bar0 = smem_u32(sm + S::BAR);
+    auto gfull = [&](int b) { return bar0 + 8 * b; };
+    auto full = [&](int b) { return bar0 + 16 + 8 * b; };
+    auto done = [&](int b) { return bar0 + 32 + 8 * b; };
+    auto wait = [&](uint32_t bar, uint32_t parity) -> bool {
+        if (*sAbort) return false;
+        if (mbar_try(bar, parity)) return true;
+        const unsigned long long t0 = gtimer();
+        while (true) {
+            if (mbar_try(bar, parity)) return true;
+            if (*sAbort || gtimer() - t0 > WAIT_NS) {
+                *sAbort = 1;
+                return false;
+            }
+        }
+    };
+
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int2 tile = a.tiles[blockIdx.x];
+    const int m = tile.x, lbase = a.blo + 1 + tile.y * SYN_ROWS;
+    const int bl = a.bl;
+    const int MH = min(lbase + SYN_ROWS - 1, bl - 1);
+    const int ctop = MH / MC;
+    const int nck = ctop + 1;  // chunks ctop, ctop-1, ..., 0
+
+    if (t == 0) {
+        for (int i = 0; i < 2; i++) {
+            mbar_init(gfull(i), 4);
+            mbar_init(full(i), 1);
+            mbar_init(done(i), 1);
+        }
+        mbar_fence_init();
+        *sAbort = 0;
+    }
+    if (warp == 0) {
+        tmem_alloc(smem_u32(sTm), TMEM_COLS);
+        tmem_relinquish();
+    }
+    if (t < COLS) {
+        const int Ef = a.vexp[(size_t)m * COLS + t];
+        sFc[t] = Ef > E_MIN ? pow2i(Ef - SHIFT) : 0.0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *sTm;
+
+    if (warp < 4) {
+        // ================= walkers / cutters =================
+        const int l = lbase + t;
+        const bool valid = l < bl && m <= l;
+        Chain cn = syn_chain_init(a.Ee, a.Em, a.B, l, m, valid);
+        const int Er = valid ? (int)a.sexp[(size_t)m * bl + l] : E_ZERO;
+        const double dfac = digit_factor(Er);
+        const double mm = (double)m;
+        double *TBp = reinterpret_cast<double *>(sm + S::TB);
+        // this lane's table rows of chunk c -> buffer b (lane-private)
+        auto stage = [&](int c, int b) {
+            double *T = TBp + b * S::T_DBL;
+            const int m0 = c * MC;
+            double *db = T + S::T_B + t * RS;
+            for (int x = 0; x < MC; x += 2) {
+                if (l < bl && m0 + x < a.Bp) cp_async16(db + x, a.Bcoef + (size_t)l * a.Bp + m0 + x);
+                else { db[x] = 0.0; db[x + 1] = 0.0; }
+            }
+            for (int q = 0; q < NP; q++) {
+                double *dg = T + S::T_G + (t * NP + q) * RS;
+                for (int x = 0; x < MC; x += 2) {
+                    if (valid && m0 + x < a.Gs)
+                        cp_async16(dg + x, a.G + ((size_t)(l - a.blo - 1) * NP + q) * a.Gs + m0 + x);
+                    else { dg[x] = 0.0; dg[x + 1] = 0.0; }
+                }
+            }
+        };
+        stage(ctop, 0);
+        cp_commit_all();
+        for (int k = 0; k < nck; k++) {
+            const int c = ctop - k, tb = k & 1;
+            if (k + 1 < nck) stage(c - 1, tb ^ 1);
+            cp_commit_all();
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            const double *T = TBp + tb * S::T_DBL;
+            // walk m' = MC c + MC - 1 .. MC c (down), values v(m', q)
+            double vals[KC];
+#pragma unroll
+            for (int i = 0; i < KC; i++) vals[i] = 0.0;
+#pragma unroll
+            for (int u = MC - 1; u >= 0; u -= 2) {
+                const double2 bb = *reinterpret_cast<const double2 *>(T + S::T_B + t * RS + u - 1);
+                double2 gg[NP];
+#pragma unroll
+                for (int q = 0; q < NP; q++)
+                    gg[q] = *reinterpret_cast<const double2 *>(T + S::T_G + (t * NP + q) * RS + u - 1);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int uu = u - h, mp = c * MC + uu;
+                    if (mp <= MH) {
+                        const double w = syn_chain_step(cn, mp, mm * (h == 0 ? bb.y : bb.x));
+#pragma unroll
+                        for (int q = 0; q < NP; q++) vals[uu * NPQ + q] = w * (h == 0 ? gg[q].y : gg[q].x);
+                        if ((mp & 15) == 0) chain_renorm(cn);
+                    }
+                }
+            }
+            if (k >= 2) wait(done(k & 1), ((k - 2) >> 1) & 1);  // MMAs of chunk k-2 finished
+            if (!*sAbort) {
+                unsigned char *gen = sm + S::GEN + (k & 1) * DIG * A_TILE;
+#pragma unroll
+                for (int kh = 0; kh < 2; kh++) {
+                    long long X[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) X[i] = to_fixed(vals[16 * kh + i], dfac);
+                    store_digits(gen + tile_off(ROWS, t, kh), A_TILE, X);
+                }
+                fence_async_smem();
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(gfull(k & 1));
+        }
+        cp_wait_all();
+    } else if (warp == ISSUER_WARP && lane == 0) {
+        // ================= issuer =================
+        auto map_copy = [&](int c, int st) {
+            mbar_expect_tx(full(st), DIG * B_TILE);
+            bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE), a.vdig + ((size_t)m * a.nch + c) * DIG * B_TILE,
+                     DIG * B_TILE, full(st));
+        };
+        const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
+                       idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
+        bool first_lev[LEV];
+#pragma unroll
+        for (int i = 0; i < LEV; i++) first_lev[i] = true;
+        map_copy(ctop, 0);
+        for (int k = 0; k < nck; k++) {
+            const int gs = k & 1, c = ctop - k;
+            if (!wait(gfull(gs), (k >> 1) & 1)) continue;
+            if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
+            if (k + 1 < nck) map_copy(c - 1, gs ^ 1);
+            if (!wait(full(gs), (k >> 1) & 1)) continue;
+            tc_fence_after();
+            const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
+            const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
+#pragma unroll
+            for (int i = 0; i < DIG; i++)
+#pragma unroll
+                for (int j = 0; j < DIG; j++) {
+                    const int lev = 2 * (DIG - 1) - i - j;
+                    if (lev >= LEV) continue;
+                    const uint32_t id = (i == DIG - 1) ? (j == DIG - 1 ? idesc_ss : idesc_su)
+                                                       : (j == DIG - 1 ? idesc_us : idesc_uu);
+                    mma_i8(tmem + lev * COLS, da0 + (uint64_t)((i * A_TILE) >> 4),
+                           db0 + (uint64_t)((j * B_TILE) >> 4), id, first_lev[lev] ? 0u : 1u);
+                    first_lev[lev] = false;
+                }
+            mma_commit(done(gs));
+        }
+        wait(done((nck - 1) & 1), ((nck - 1) >> 1) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    const bool abort = *sAbort != 0;
+    if (abort && t == 0) atomicExch(a.err, 1);
+
+    // ---- epilogue: warp w reads rows 32*(w&3).. and columns [32*(w>>2), +32)
+    {
+        const int row = 32 * (warp & 3) + lane, half = warp >> 2;
+        const int l = lbase + row;
+        const bool valid = l < bl && m <= l;
+        const int Er = valid ? (int)a.sexp[(size_t)m * bl + l] : E_ZERO;
+        const double rowf = Er > E_MIN ? pow2i(Er) : 0.0;
+        for (int blk = 0; blk < 2; blk++) {
+            const int col0 = 32 * half + 16 * blk;
+            double acc[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) acc[i] = 0.0;
+            if (!abort) {
+#pragma unroll
+                for (int lev = 0; lev < LEV; lev++) {
+                    int32_t r[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + lev * COLS + col0, r);
+                    const double wgt = pow2i(-8 * lev);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
+                }
+            }
+            if (valid) {
+#pragma unroll
+                for (int i = 0; i < 16; i += 2) {
+                    const int k = (col0 + i) >> 1;
+                    if (k < a.nmaps) {
+                        const double2 z = make_double2((acc[i] * rowf) * sFc[col0 + i], (acc[i + 1] * rowf) * sFc[col0 + i + 1]);
+                        a.part[(size_t)k * a.pstride + (size_t)(l - a.blo - 1) * bl + m] = c_ipow(z, m);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
+}
+
 }  // namespace split
 
 int split_chains(int NP) { return split::chains(NP); }
@@ -806,6 +1147,62 @@ int launch_split(const SplitArgs &a, cudaStream_t s)
     case 2: return launch_split_t<2>(a, s);
     case 3: return launch_split_t<3>(a, s);
     default: return launch_split_t<4>(a, s);
+    }
+}
+
+
+int split_syn_mc(int NP) { return split::syn_mc(NP); }
+long long split_vdig_bytes(int bl, int nch) { return (long long)bl * nch * split::DIG * split::B_TILE; }
+
+int launch_split_syn_dexp(const SplitSynArgs &a, cudaStream_t s)
+{
+    if (a.ntiles <= 0) return S2DWC_OK;
+    switch (a.NP) {
+    case 1: split::syn_dexp_kernel<1><<<a.ntiles, split::SYN_ROWS, 0, s>>>(a); break;
+    case 2: split::syn_dexp_kernel<2><<<a.ntiles, split::SYN_ROWS, 0, s>>>(a); break;
+    case 3: split::syn_dexp_kernel<3><<<a.ntiles, split::SYN_ROWS, 0, s>>>(a); break;
+    default: split::syn_dexp_kernel<4><<<a.ntiles, split::SYN_ROWS, 0, s>>>(a); break;
+    }
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_split_vdig(const VdigArgs &a, cudaStream_t s)
+{
+    if (a.bl <= 0 || a.nch <= 0) return S2DWC_OK;
+    switch (a.NP) {
+    case 1: split::vdig_kernel<1><<<a.bl, split::THREADS, 0, s>>>(a); break;
+    case 2: split::vdig_kernel<2><<<a.bl, split::THREADS, 0, s>>>(a); break;
+    case 3: split::vdig_kernel<3><<<a.bl, split::THREADS, 0, s>>>(a); break;
+    default: split::vdig_kernel<4><<<a.bl, split::THREADS, 0, s>>>(a); break;
+    }
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+template <int NP>
+static int launch_split_syn_t(const SplitSynArgs &a, cudaStream_t s)
+{
+    const int bytes = split::SynSmem<NP>::BYTES;
+    static bool attr = false;
+    if (!attr) {
+        S2DW_CUDA_TRY(
+            cudaFuncSetAttribute(split::split_syn_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        attr = true;
+    }
+    split::split_syn_kernel<NP><<<a.ntiles, split::SPLIT_THREADS, bytes, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_split_syn(const SplitSynArgs &a, cudaStream_t s)
+{
+    if (a.ntiles <= 0) return S2DWC_OK;
+    switch (a.NP) {
+    case 1: return launch_split_syn_t<1>(a, s);
+    case 2: return launch_split_syn_t<2>(a, s);
+    case 3: return launch_split_syn_t<3>(a, s);
+    default: return launch_split_syn_t<4>(a, s);
     }
 }
 

@@ -1,11 +1,12 @@
-"""Split-precision analysis (tensor-core int8 digit contraction) against the
-FP64 analysis of the same maps, for batches of maps.
+"""Split-precision form (tensor-core int8 digit contractions) against the FP64
+form on the same maps, for batches of maps.
 
-Tolerance: per map and per scale, max|w_split - w_fp64| <= 1e-10 * max|w_fp64|
-(the split form's stated bound; its design error is ~1e-11), and the FP64
-synthesis of the split coefficients reconstructs flm within 1e-10.  Cases
-cover every size of the positive-n set (NP = 1..4), alpha = 3, a batch larger
-than one 32-map group, and a batch of one."""
+Tolerances (the split form's stated bound; its design error is ~1e-11):
+analysis, per map and per scale, max|w_split - w_fp64| <= 1e-10 * max|w_fp64|;
+synthesis of the same coefficients, max|flm_split - flm_fp64| <= 1e-10 *
+max|flm_fp64|; split analysis then split synthesis reconstructs flm within
+1e-10.  Cases cover every size of the positive-n set (NP = 1..4), alpha = 3, a
+batch larger than one 32-map group, and a batch of one."""
 import numpy as np
 import pytest
 
@@ -37,7 +38,10 @@ def _run(B, N, alpha, nmaps, seed0=100):
     split.analysis_batch(d_flm, w_sp, s_sp)
     split.check()
     out = torch.empty_like(d_flm)
-    plain.synthesis_batch(w_sp, s_sp, out)
+    out_plain = torch.empty_like(d_flm)
+    split.synthesis_batch(w_sp, s_sp, out)
+    split.check()
+    plain.synthesis_batch(w_sp, s_sp, out_plain)
     torch.cuda.synchronize()
     wr, ws = w_ref.cpu().numpy(), w_sp.cpu().numpy()
     offs = plain.wav_offsets
@@ -52,9 +56,11 @@ def _run(B, N, alpha, nmaps, seed0=100):
             worst = max(worst, np.abs(a - b).max() / scale)
     np.testing.assert_array_equal(s_sp.cpu().numpy(), s_ref.cpu().numpy())
     recon = max(np.abs(out[k].cpu().numpy().T - flms[k]).max() for k in range(nmaps))
+    fs, fp = out.cpu().numpy(), out_plain.cpu().numpy()
+    syn = max(np.abs(fs[k] - fp[k]).max() / np.abs(fp[k]).max() for k in range(nmaps))
     plain.close()
     split.close()
-    return worst, recon
+    return worst, recon, syn
 
 
 @pytest.mark.gpu
@@ -67,14 +73,16 @@ def _run(B, N, alpha, nmaps, seed0=100):
     (96, 4, 2.0, 1),    # one map
 ])
 def test_split_matches_fp64(B, N, alpha, nmaps):
-    worst, recon = _run(B, N, alpha, nmaps)
+    worst, recon, syn = _run(B, N, alpha, nmaps)
     assert worst <= TOL_W, f"max|dw|/max|w| = {worst:.3e}"
+    assert syn <= TOL_W, f"max|dflm|/max|flm| = {syn:.3e}"
     assert recon <= TOL_RECON, f"recon {recon:.3e}"
 
 
 @pytest.mark.gpu
 def test_split_b256_n5():
     """The split-form comparison configuration: B=256, N=5, alpha=2."""
-    worst, recon = _run(256, 5, 2.0, 4)
+    worst, recon, syn = _run(256, 5, 2.0, 4)
     assert worst <= TOL_W, f"max|dw|/max|w| = {worst:.3e}"
+    assert syn <= TOL_W, f"max|dflm|/max|flm| = {syn:.3e}"
     assert recon <= TOL_RECON, f"recon {recon:.3e}"
