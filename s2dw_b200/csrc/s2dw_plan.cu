@@ -75,6 +75,8 @@ struct s2dwc_plan {
         int snch = 0, sntiles = 0;
         int2 *stiles = nullptr;
         long long sexp_off = 0;
+        // per-scale workspaces (offsets in elements of the buffers below)
+        long long fdig_off = 0, vdig_off = 0, fexp_off = 0, tg_off = 0, tb_off = 0, v2f_off = 0, vstride = 0;
     };
     std::vector<SplitScale> sp;
     bool sp_alloc = false, sp_dexp_valid = false;
@@ -86,7 +88,7 @@ struct s2dwc_plan {
     int32_t *sp_vexp = nullptr;
     uint8_t *sp_vdig = nullptr;
     double2 *sp_V2f = nullptr, *sp_part = nullptr;
-    long long sp_vstride = 0, sp_pstride = 0;
+    long long sp_pstride = 0;
     int *sp_err = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
@@ -612,26 +614,41 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
     return launch_scoeff_copy(d_scoeff, d_flm, p->B, p->bl_scoeff, s);
 }
 
-// Split form: workspaces, tile lists and the per-row exponent tables (the
+// Split form: per-scale workspaces (the scales of a batch run concurrently
+// on the plan's streams), tile lists and the per-row exponent tables (the
 // latter depend on the kernel tables and are rebuilt after set_tables).
 int split_prepare(s2dwc_plan *p, cudaStream_t s)
 {
     int st;
-    const int NP = p->NP, CH = split_chains(NP), MAPS = split_maps_per_pass();
+    const int NP = p->NP, CH = split_chains(NP), MAPS = split_maps_per_pass(), MC = split_syn_mc(NP);
     if (!p->sp_alloc) {
         p->sp.resize(p->J + 1);
-        long long nd = 0, fdig = 0;
-        int blmax = 0;
+        long long nd = 0, ns = 0, fdig = 0, fexp = 0, tg = 0, tb = 0, v2f = 0, vdig = 0;
         for (int j = 0; j <= p->J; j++) {
             auto &S = p->sp[j];
-            const int bl = p->bl[j], blo = p->blo[j];
-            blmax = std::max(blmax, bl);
+            const int bl = p->bl[j], blo = p->blo[j], nl = bl - blo - 1;
+            const long long Vs = p->gs_stride[j];
             S.c0 = (blo + 1) / 32;
             S.nch = (bl - 1) / 32 - S.c0 + 1;
+            S.snch = (bl + MC - 1) / MC;
             S.dexp_off = nd;
             nd += (long long)bl * bl * NP;
-            fdig = std::max(fdig, split_fdig_bytes(bl, S.nch));
-            // (m, chain tile), longest walks (smallest first row) first
+            S.sexp_off = ns;
+            ns += (long long)bl * bl;
+            S.fdig_off = fdig;
+            fdig += (split_fdig_bytes(bl, S.nch) + 255) / 256 * 256;
+            S.vdig_off = vdig;
+            vdig += (split_vdig_bytes(bl, S.snch) + 255) / 256 * 256;
+            S.fexp_off = fexp;
+            fexp += (long long)bl * 64;
+            S.tg_off = tg;
+            tg += (long long)MAPS * p->N * bl * bl;
+            S.tb_off = tb;
+            tb += (long long)p->N * bl * 2 * bl;
+            S.vstride = (long long)NP * bl * Vs;
+            S.v2f_off = v2f;
+            v2f += MAPS * S.vstride;
+            // analysis tiles (m, chain tile), longest walks (smallest first row) first
             std::vector<int2> tl;
             const int np = (bl + CH - 1) / CH;
             for (int m = 0; m < bl; m++)
@@ -641,19 +658,9 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             });
             S.ntiles = (int)tl.size();
             if ((st = dev_upload(p, &S.tiles, tl))) return st;
-        }
-        // synthesis: (m, 128-row l tile) tiles, m-major so that the tiles of one m
-        // share the map digits in L2
-        long long ns = 0, vdig = 0;
-        const int MC = split_syn_mc(NP);
-        for (int j = 0; j <= p->J; j++) {
-            auto &S = p->sp[j];
-            const int bl = p->bl[j], blo = p->blo[j], nl = bl - blo - 1;
-            S.snch = (bl + MC - 1) / MC;
-            S.sexp_off = ns;
-            ns += (long long)bl * bl;
-            vdig = std::max(vdig, split_vdig_bytes(bl, S.snch));
-            std::vector<int2> tl;
+            // synthesis tiles (m, 128-row l tile), m-major so that the tiles of
+            // one m share its map digits in L2
+            tl.clear();
             for (int m = 0; m < bl; m++)
                 for (int lt = 0; lt * 128 < nl; lt++) {
                     const int lbase = blo + 1 + lt * 128;
@@ -663,18 +670,13 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             if (tl.empty()) tl.push_back(make_int2(0, 0));
             if ((st = dev_upload(p, &S.stiles, tl))) return st;
         }
-        p->sp_vstride = (long long)p->NP * blmax * ((blmax + 7) / 8 * 8);
         p->sp_pstride = std::max(1LL, p->offP.back() + (long long)std::max(0, p->bl[p->J] - p->blo[p->J] - 1) * p->bl[p->J]);
-        if ((st = dev_alloc(p, &p->sp_sexp, (size_t)ns)) || (st = dev_alloc(p, &p->sp_vexp, (size_t)blmax * 64)) ||
-            (st = dev_alloc(p, &p->sp_vdig, (size_t)vdig)) ||
-            (st = dev_alloc(p, &p->sp_V2f, (size_t)MAPS * p->sp_vstride)) ||
-            (st = dev_alloc(p, &p->sp_part, (size_t)MAPS * p->sp_pstride)))
-            return st;
-        const long long b2 = (long long)blmax * blmax;
-        if ((st = dev_alloc(p, &p->sp_dexp, (size_t)nd)) || (st = dev_alloc(p, &p->sp_fexp, (size_t)blmax * 64)) ||
-            (st = dev_alloc(p, &p->sp_fdig, (size_t)fdig)) ||
-            (st = dev_alloc(p, &p->sp_Tg, (size_t)MAPS * p->N * b2)) ||
-            (st = dev_alloc(p, &p->sp_Tb, (size_t)p->N * 2 * b2)) || (st = dev_alloc(p, &p->sp_err, 1)))
+        if ((st = dev_alloc(p, &p->sp_dexp, (size_t)nd)) || (st = dev_alloc(p, &p->sp_sexp, (size_t)ns)) ||
+            (st = dev_alloc(p, &p->sp_fexp, (size_t)fexp)) || (st = dev_alloc(p, &p->sp_vexp, (size_t)fexp)) ||
+            (st = dev_alloc(p, &p->sp_fdig, (size_t)fdig)) || (st = dev_alloc(p, &p->sp_vdig, (size_t)vdig)) ||
+            (st = dev_alloc(p, &p->sp_Tg, (size_t)tg)) || (st = dev_alloc(p, &p->sp_Tb, (size_t)tb)) ||
+            (st = dev_alloc(p, &p->sp_V2f, (size_t)v2f)) ||
+            (st = dev_alloc(p, &p->sp_part, (size_t)MAPS * p->sp_pstride)) || (st = dev_alloc(p, &p->sp_err, 1)))
             return st;
         S2DW_CUDA_TRY(cudaMemsetAsync(p->sp_err, 0, sizeof(int), s));
         // gamma-DFT phases exp(i pi n g / N), [g*16 + n+N-1]
@@ -729,10 +731,32 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
     return S2DWC_OK;
 }
 
+// Runs f(j, stream) for every scale: on the plan's per-scale streams forked
+// from and joined back to `s`, or all on `s` in timing mode.
+template <typename F>
+int for_scales(s2dwc_plan *p, cudaStream_t s, F &&f)
+{
+    int st;
+    if (p->timing) {
+        for (int j = 0; j <= p->J; j++)
+            if ((st = f(j, s))) return st;
+        return S2DWC_OK;
+    }
+    S2DW_CUDA_TRY(cudaEventRecord(p->ev_fork, s));
+    for (int j = 0; j <= p->J; j++) {
+        S2DW_CUDA_TRY(cudaStreamWaitEvent(p->streams[j], p->ev_fork, 0));
+        if ((st = f(j, p->streams[j]))) return st;
+        S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], p->streams[j]));
+    }
+    for (int j = 0; j <= p->J; j++) S2DW_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[j], 0));
+    return S2DWC_OK;
+}
+
 // Split-form analysis of `nmaps` maps (flm, wav and scoeff of map k at
-// k * B^2, k * wav_total and k * bl_scoeff^2): per group of up to 32 maps
-// and per scale, the map digits, the tensor-core contraction into Tg of the
-// whole group, then the beta and alpha transforms map by map.
+// k * B^2, k * wav_total and k * bl_scoeff^2): per group of up to 32 maps,
+// every scale on its own stream runs the map digits, the tensor-core
+// contraction into Tg of the whole group, then the beta and alpha transforms
+// map by map.
 int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoeff, const double2 *d_flm,
                        cudaStream_t s)
 {
@@ -743,7 +767,8 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
     const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
     for (int g0 = 0; g0 < nmaps; g0 += MAPS) {
         const int nk = std::min(MAPS, nmaps - g0);
-        for (int j = 0; j <= p->J; j++) {
+        st = for_scales(p, s, [&](int j, cudaStream_t sj) -> int {
+            int st2;
             const int bl = p->bl[j];
             const auto &S = p->sp[j];
             FdigArgs fa{};
@@ -754,11 +779,11 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             fa.nch = S.nch;
             fa.nmaps = nk;
             fa.flm = d_flm + g0 * B2;
-            fa.fexp = p->sp_fexp;
-            fa.fdig = p->sp_fdig;
+            fa.fexp = p->sp_fexp + S.fexp_off;
+            fa.fdig = p->sp_fdig + S.fdig_off;
             {
-                KernelTimer kt(p, S2DWC_KIND_OTHER, s);
-                if ((st = launch_split_fdig(fa, s))) return st;
+                KernelTimer kt(p, S2DWC_KIND_OTHER, sj);
+                if ((st2 = launch_split_fdig(fa, sj))) return st2;
             }
             SplitArgs a{};
             a.B = p->B;
@@ -778,16 +803,16 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             a.G = p->Ga + p->ga_off[j];
             a.Gs = p->ga_stride[j];
             a.dexp = p->sp_dexp + S.dexp_off;
-            a.fexp = p->sp_fexp;
-            a.fdig = p->sp_fdig;
-            a.Tg = p->sp_Tg;
+            a.fexp = p->sp_fexp + S.fexp_off;
+            a.fdig = p->sp_fdig + S.fdig_off;
+            a.Tg = p->sp_Tg + S.tg_off;
             a.ph = p->sp_ph;
             a.tiles = S.tiles;
             a.ntiles = S.ntiles;
             a.err = p->sp_err;
             {
-                KernelTimer kt(p, S2DWC_KIND_LWALK, s);
-                if ((st = launch_split(a, s))) return st;
+                KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
+                if ((st2 = launch_split(a, sj))) return st2;
             }
             for (int k = 0; k < nk; k++) {
                 CztArgs ca{};
@@ -799,24 +824,26 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
                 ca.rows = p->N * bl;
                 ca.czt = p->czt[j][ca.mode];
                 ca.tw = p->tw.at(ca.czt.M);
-                ca.in_c = p->sp_Tg + (long long)k * p->N * bl * bl;
-                ca.out_c = p->sp_Tb;
+                ca.in_c = p->sp_Tg + S.tg_off + (long long)k * p->N * bl * bl;
+                ca.out_c = p->sp_Tb + S.tb_off;
                 {
-                    KernelTimer kt(p, S2DWC_KIND_ANA_BETA, s);
-                    if ((st = launch_czt(ca, s))) return st;
+                    KernelTimer kt(p, S2DWC_KIND_ANA_BETA, sj);
+                    if ((st2 = launch_czt(ca, sj))) return st2;
                 }
                 ca.mode = CZT_ANA_ALPHA;
                 ca.czt = p->czt[j][CZT_ANA_ALPHA];
                 ca.tw = p->tw.at(ca.czt.M);
-                ca.in_c = p->sp_Tb;
+                ca.in_c = p->sp_Tb + S.tb_off;
                 ca.out_c = nullptr;
                 ca.out_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
                 {
-                    KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, s);
-                    if ((st = launch_czt(ca, s))) return st;
+                    KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, sj);
+                    if ((st2 = launch_czt(ca, sj))) return st2;
                 }
             }
-        }
+            return S2DWC_OK;
+        });
+        if (st) return st;
         for (int k = 0; k < nk; k++) {
             KernelTimer kt(p, S2DWC_KIND_OTHER, s);
             if ((st = launch_scoeff_copy(d_scoeff ? d_scoeff + (g0 + k) * bs2 : nullptr, d_flm + (g0 + k) * B2, p->B,
@@ -828,9 +855,10 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
 }
 
 // Split-form synthesis of `nmaps` maps (layouts as run_analysis_split): per
-// group of up to 32 maps and per scale, the alpha and beta transforms map by
-// map into a batch of V tables, their digits, the tensor-core contraction
-// into per-map partial rows; then the scale sum of each map.
+// group of up to 32 maps, every scale on its own stream runs the alpha and
+// beta transforms map by map into a batch of V tables, their digits and the
+// tensor-core contraction into per-map partial rows; then the scale sum of
+// each map, scales in order.
 int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *d_wav, const double2 *d_scoeff,
                         cudaStream_t s)
 {
@@ -841,7 +869,8 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
     const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
     for (int g0 = 0; g0 < nmaps; g0 += MAPS) {
         const int nk = std::min(MAPS, nmaps - g0);
-        for (int j = 0; j <= p->J; j++) {
+        st = for_scales(p, s, [&](int j, cudaStream_t sj) -> int {
+            int st2;
             const int bl = p->bl[j];
             const auto &S = p->sp[j];
             for (int k = 0; k < nk; k++) {
@@ -855,40 +884,40 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
                 ca.czt = p->czt[j][CZT_SYN_ALPHA];
                 ca.tw = p->tw.at(ca.czt.M);
                 ca.in_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
-                ca.out_c = p->sp_Tb;
+                ca.out_c = p->sp_Tb + S.tb_off;
                 ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
                 {
-                    KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, s);
-                    if ((st = launch_czt(ca, s))) return st;
+                    KernelTimer kt(p, S2DWC_KIND_SYN_ALPHA, sj);
+                    if ((st2 = launch_czt(ca, sj))) return st2;
                 }
                 ca.mode = p->syn_beta_mode[j];
                 ca.rows = p->NP * bl;
                 ca.czt = p->czt[j][ca.mode];
                 ca.tw = p->tw.at(ca.czt.M);
-                ca.in_c = p->sp_Tb;
+                ca.in_c = p->sp_Tb + S.tb_off;
                 ca.in_r = nullptr;
-                ca.out_c = p->sp_V2f + k * p->sp_vstride;
+                ca.out_c = p->sp_V2f + S.v2f_off + k * S.vstride;
                 ca.out_stride = p->gs_stride[j];
                 ca.wq = p->wq[j];
                 {
-                    KernelTimer kt(p, S2DWC_KIND_SYN_BETA, s);
-                    if ((st = launch_czt(ca, s))) return st;
+                    KernelTimer kt(p, S2DWC_KIND_SYN_BETA, sj);
+                    if ((st2 = launch_czt(ca, sj))) return st2;
                 }
             }
-            if (bl - p->blo[j] - 1 <= 0) continue;
+            if (bl - p->blo[j] - 1 <= 0) return S2DWC_OK;
             VdigArgs va{};
             va.bl = bl;
             va.NP = p->NP;
             va.nch = S.snch;
             va.nmaps = nk;
             va.Vs = p->gs_stride[j];
-            va.V2f = p->sp_V2f;
-            va.vstride = p->sp_vstride;
-            va.vexp = p->sp_vexp;
-            va.vdig = p->sp_vdig;
+            va.V2f = p->sp_V2f + S.v2f_off;
+            va.vstride = S.vstride;
+            va.vexp = p->sp_vexp + S.fexp_off;
+            va.vdig = p->sp_vdig + S.vdig_off;
             {
-                KernelTimer kt(p, S2DWC_KIND_OTHER, s);
-                if ((st = launch_split_vdig(va, s))) return st;
+                KernelTimer kt(p, S2DWC_KIND_OTHER, sj);
+                if ((st2 = launch_split_vdig(va, sj))) return st2;
             }
             SplitSynArgs b{};
             b.B = p->B;
@@ -905,18 +934,17 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
             b.G = p->Gsyn + p->gs_off[j];
             b.Gs = p->gs_stride[j];
             b.sexp = p->sp_sexp + S.sexp_off;
-            b.vexp = p->sp_vexp;
-            b.vdig = p->sp_vdig;
+            b.vexp = p->sp_vexp + S.fexp_off;
+            b.vdig = p->sp_vdig + S.vdig_off;
             b.part = p->sp_part + p->offP[j];
             b.pstride = p->sp_pstride;
             b.tiles = S.stiles;
             b.ntiles = S.sntiles;
             b.err = p->sp_err;
-            {
-                KernelTimer kt(p, S2DWC_KIND_MWALK, s);
-                if ((st = launch_split_syn(b, s))) return st;
-            }
-        }
+            KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
+            return launch_split_syn(b, sj);
+        });
+        if (st) return st;
         for (int k = 0; k < nk; k++) {
             CombineArgs cb{};
             cb.B = p->B;
