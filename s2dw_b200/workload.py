@@ -73,17 +73,16 @@ def run_pairs(B, N, alpha=2.0, pairs=2, seed=0):
 
 def run_batch(B, N, alpha=2.0, maps=32, form=1, repeats=1):
     """Runs `repeats` batched analyses of `maps` seeded maps through a plan of
-    `form` (0 FP64, 1 split) on cuda:0, then one FP64 synthesis of the last
-    batch; returns the worst reconstruction error over the maps."""
+    `form` (0 FP64, 1 split) on cuda:0, then one batched synthesis of the last
+    batch through the same plan; returns the worst reconstruction error over
+    the maps."""
     import torch
 
     from .device import Plan
 
     t = transform_setup(B, N, alpha)
     plan = Plan(B, N, alpha, t["J"], form=form)
-    syn = Plan(B, N, alpha, t["J"])
-    for p in (plan, syn):
-        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    plan.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
     flms = [gaussian_flm(B, seed=k) for k in range(maps)]
     d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
     d_wav = torch.empty((maps, plan.wav_size), dtype=torch.float64, device="cuda")
@@ -92,11 +91,11 @@ def run_batch(B, N, alpha=2.0, maps=32, form=1, repeats=1):
         plan.analysis_batch(d_flm, d_wav, d_sc)
     plan.check()
     d_out = torch.empty_like(d_flm)
-    syn.synthesis_batch(d_wav, d_sc, d_out)
+    plan.synthesis_batch(d_wav, d_sc, d_out)
+    plan.check()
     torch.cuda.synchronize()
     err = max(float(np.abs(d_out[k].cpu().numpy().T - flms[k]).max()) for k in range(maps))
     plan.close()
-    syn.close()
     return err
 
 
@@ -108,6 +107,6 @@ if __name__ == "__main__":
     a = [int(x) for x in sys.argv[1:5]] + [None] * 4
     B, N, P, M = a[0] or 1024, a[1] or 4, a[2] or 2, a[3]
     if M:
-        print(f"B={B} N={N} maps={M} split analyses={P} recon {run_batch(B, N, 2.0, M, 1, P):.3e}")
+        print(f"B={B} N={N} maps={M} split analyses={P} + synthesis, recon {run_batch(B, N, 2.0, M, 1, P):.3e}")
     else:
         print(f"B={B} N={N} pairs={P} recon {run_pairs(B, N, 2.0, P):.3e}")
