@@ -13,6 +13,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -384,7 +385,13 @@ struct KernelTimer {
 
 // Runs the analysis: the F table on `s`, then every scale on its own stream
 // (forked from and joined back to `s`).
-int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s)
+// Per-scale hook: enqueued on scale j's stream after (analysis) or before
+// (synthesis) that scale's kernels; the host-buffer entry points use it to
+// overlap each scale's host<->device copy with the other scales' kernels.
+using ScaleHook = std::function<int(int, cudaStream_t)>;
+
+int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s,
+                 const ScaleHook &after = ScaleHook())
 {
     int st;
     {
@@ -446,6 +453,7 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
             KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, sj);
             if ((st = launch_czt(ca, sj))) return st;
         }
+        if (after && (st = after(j, sj))) return st;
         if (!p->timing) S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], sj));
     }
     {
@@ -458,13 +466,14 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
 }
 
 int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const double2 *d_scoeff,
-                  cudaStream_t s)
+                  cudaStream_t s, const ScaleHook &before = ScaleHook())
 {
     int st;
     S2DW_CUDA_TRY(cudaEventRecord(p->ev_fork, s));
     for (int j = 0; j <= p->J; j++) {
         cudaStream_t sj = p->timing ? s : p->streams[j];
         if (!p->timing) S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_fork, 0));
+        if (before && (st = before(j, sj))) return st;
         const int bl = p->bl[j];
         double2 *Vw = p->wsA + p->offA[j], *V2f = p->wsC + p->offC[j];
         CztArgs ca{};
@@ -1319,6 +1328,21 @@ static int host_prepare(int B, int N, double alpha, int J, int bl_scoeff, const 
     return S2DWC_OK;
 }
 
+// True when every pointer is page-locked host memory: then per-scale copies
+// can be queued asynchronously on the scales' streams without blocking the
+// host thread that queues the kernels.
+static bool all_pinned(const void *const *ptrs, int n)
+{
+    for (int i = 0; i < n; i++) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ptrs[i]) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            return false;
+        }
+    }
+    return true;
+}
+
 static int analysis_host(double *wav_static, double *const *wav_scales, double *scoeff, const double *flm,
                          const double *K_gamma, const double *Slm, int J, int B, int N, int bl_scoeff,
                          double alpha)
@@ -1332,11 +1356,24 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
     std::lock_guard<std::mutex> g(p->mu);
     DeviceGuard dg(p->device);
     S2DW_CUDA_TRY(cudaMemcpy(hb.flm, flm, sizeof(double2) * (size_t)B * B, cudaMemcpyHostToDevice));
-    if ((st = run_analysis(p, hb.wav, hb.sc, hb.flm, 0))) return st;
+    // pinned per-scale outputs: each scale's device-to-host copy follows its
+    // kernels on its stream and overlaps the other scales
+    const bool overlap = wav_scales && all_pinned(reinterpret_cast<const void *const *>(wav_scales), J + 1);
+    ScaleHook copy_out;
+    if (overlap)
+        copy_out = [&](int j, cudaStream_t sj) -> int {
+            S2DW_CUDA_TRY(cudaMemcpyAsync(wav_scales[j], hb.wav + p->wav_off[j],
+                                          sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
+                                          cudaMemcpyDeviceToHost, sj));
+            return S2DWC_OK;
+        };
+    if ((st = run_analysis(p, hb.wav, hb.sc, hb.flm, 0, copy_out))) return st;
     if (bl_scoeff > 0)
         S2DW_CUDA_TRY(cudaMemcpy(scoeff, hb.sc, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
                                  cudaMemcpyDeviceToHost));
-    if (wav_scales) {
+    if (overlap) {
+        S2DW_CUDA_TRY(cudaStreamSynchronize(0));
+    } else if (wav_scales) {
         for (int j = 0; j <= J; j++)
             S2DW_CUDA_TRY(cudaMemcpy(wav_scales[j], hb.wav + p->wav_off[j],
                                      sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
@@ -1390,7 +1427,18 @@ static int synthesis_host(double *flm, const double *wav_static, const double *c
     if (st) return st;
     std::lock_guard<std::mutex> g(p->mu);
     DeviceGuard dg(p->device);
-    if (wav_scales) {
+    // pinned per-scale inputs: each scale's host-to-device copy precedes its
+    // kernels on its stream and overlaps the other scales
+    const bool overlap = wav_scales && all_pinned(reinterpret_cast<const void *const *>(wav_scales), J + 1);
+    ScaleHook copy_in;
+    if (overlap) {
+        copy_in = [&](int j, cudaStream_t sj) -> int {
+            S2DW_CUDA_TRY(cudaMemcpyAsync(hb.wav + p->wav_off[j], wav_scales[j],
+                                          sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
+                                          cudaMemcpyHostToDevice, sj));
+            return S2DWC_OK;
+        };
+    } else if (wav_scales) {
         for (int j = 0; j <= J; j++)
             S2DW_CUDA_TRY(cudaMemcpy(hb.wav + p->wav_off[j], wav_scales[j],
                                      sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
@@ -1412,7 +1460,7 @@ static int synthesis_host(double *flm, const double *wav_static, const double *c
     if (bl_scoeff > 0)
         S2DW_CUDA_TRY(cudaMemcpy(hb.sc, scoeff, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
                                  cudaMemcpyHostToDevice));
-    if ((st = run_synthesis(p, hb.flm, hb.wav, hb.sc, 0))) return st;
+    if ((st = run_synthesis(p, hb.flm, hb.wav, hb.sc, 0, copy_in))) return st;
     S2DW_CUDA_TRY(cudaMemcpy(flm, hb.flm, sizeof(double2) * (size_t)B * B, cudaMemcpyDeviceToHost));
     return S2DWC_OK;
 }

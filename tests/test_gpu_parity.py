@@ -153,3 +153,43 @@ def test_device_plan_matches_host_api():
     f = d_out.cpu().numpy().T
     assert np.abs(f - flm).max() < 1e-12
     plan.close()
+
+
+@pytest.mark.gpu
+def test_host_api_pinned_buffers_match_pageable():
+    """Page-locked per-scale buffers take the path whose copies overlap the
+    scales' kernels; the results are the same as with pageable buffers."""
+    import ctypes
+
+    import torch
+
+    from s2dw_b200._lib import check, lib
+
+    B, N, alpha = 128, 4, 2.0
+    t = transform_setup(B, N, alpha)
+    J, bs = t["J"], t["bl_scoeff"]
+    flm = gaussian_flm(B, seed=9)
+    a = (t["K_gamma"], t["Slm"], J, B, N, bs, alpha)
+    wav_ref, sc_ref = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+    dp = ctypes.POINTER(ctypes.c_double)
+    shapes = [core.wav_scale_shape(j, B, N, alpha) for j in range(J + 1)]
+    wav_p = [torch.empty(s[::-1], dtype=torch.float64, pin_memory=True).numpy().T for s in shapes]
+    wptr = (dp * (J + 1))(*[w.ctypes.data_as(dp) for w in wav_p])
+    sc = np.zeros((bs, bs), dtype=np.complex128, order="F")
+    K = np.asfortranarray(t["K_gamma"])
+    S = np.asfortranarray(t["Slm"])
+    f = np.asfortranarray(flm)
+    check(lib().s2dwc_analysis_flm2wav_dynamic(wptr, sc.ctypes.data_as(dp), f.ctypes.data_as(dp),
+                                               K.ctypes.data_as(dp), S.ctypes.data_as(dp), J, B, N, bs, alpha))
+    for j in range(J + 1):
+        np.testing.assert_array_equal(wav_p[j], wav_ref[j])
+    np.testing.assert_array_equal(sc, sc_ref)
+    out = torch.empty((B, B), dtype=torch.complex128, pin_memory=True).numpy().T
+    P = np.ascontiguousarray(t["Phi2"])
+    check(lib().s2dwc_synthesis_wav2flm_dynamic(out.ctypes.data_as(dp), wptr, sc.ctypes.data_as(dp),
+                                                K.ctypes.data_as(dp), P.ctypes.data_as(dp), S.ctypes.data_as(dp),
+                                                J, B, N, bs, alpha))
+    ref = core.s2dw_core_synthesis_wav2flm_dynamic(wav_ref, sc_ref, t["K_gamma"], t["Phi2"], t["Slm"], J, B, N,
+                                                   bs, alpha)
+    np.testing.assert_array_equal(out, ref)
+    assert np.abs(out - flm).max() < 1e-12
