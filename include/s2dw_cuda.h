@@ -54,14 +54,14 @@ extern "C" {
 #define S2DWC_ERROR_CUDA 15
 
 /* Precision form of the transform.  FP64: every stage in FP64, the drop-in
- * form.  SPLIT: the analysis contraction runs on the tensor cores as exact
- * int8 products of 48-bit fixed-point digits (six byte digits per operand,
- * per-row and per-column power-of-two scales, the 28 most significant digit
- * products summed exactly in int32), combined in FP64; the d^l(pi/2)
- * recurrence, the kernel tables and the beta/alpha transforms stay FP64, and
- * synthesis is the FP64 one.  Its analysis error is bounded by 1e-10 of
- * max|w| per scale; it pays off for batches of maps
- * (s2dwc_plan_analysis_batch), which share the d-operand. */
+ * form.  SPLIT: the analysis and synthesis contractions run on the tensor
+ * cores as exact int8 products of 48-bit fixed-point digits (six byte digits
+ * per operand, per-row and per-column power-of-two scales, the 28 most
+ * significant digit products summed exactly in int32), combined in FP64; the
+ * d^l(pi/2) recurrences, the kernel tables and the beta/alpha transforms stay
+ * FP64.  Its error is bounded by 1e-10 of max|w| per scale (analysis) and of
+ * max|flm| (synthesis); it pays off for batches of maps
+ * (s2dwc_plan_analysis_batch / _synthesis_batch), which share the d-operand. */
 #define S2DWC_FORM_FP64 0
 #define S2DWC_FORM_SPLIT 1
 
@@ -192,6 +192,29 @@ int s2dwc_plan_analysis_batch(s2dwc_plan *plan, int nmaps, double *d_wav, double
                               const double *d_flm, void *stream);
 int s2dwc_plan_synthesis_batch(s2dwc_plan *plan, int nmaps, double *d_flm, const double *d_wav,
                                const double *d_scoeff, void *stream);
+
+/* Moments of the wavelet coefficients per scale for `nmaps` device-resident
+ * maps in the packed layout (map k at d_wav + k*offsets[J+1]): the
+ * computation of s2dw_stat_moments (src/mod/s2dw_stat_mod.f90:81-275) without
+ * copying the coefficients to the host, as the reference's s2dw_wstats needs
+ * (src/prog/s2dw_wstats.f90:181-197).  d_mask is one map's packed mask (the
+ * same for every map) or NULL.  d_moments receives nmaps*(J+1)*6 doubles,
+ * [map][scale][mean, var, skew, kur, five, six]; scales with zero variance
+ * get zero higher moments, scales with fewer than two samples get zeros.
+ * Unlike the reference, d_wav is not masked in place. */
+int s2dwc_plan_stat_moments(s2dwc_plan *plan, int nmaps, const double *d_wav, const double *d_mask,
+                            double *d_moments, void *stream);
+
+/* Replaces s2dw_stat_moments, src/mod/s2dw_stat_mod.f90:81-275: host per-scale
+ * arrays (the dynamic layout), the reference's argument order.  mask_scales,
+ * five and six may be NULL (the reference's optional arguments); with a mask
+ * the coefficients are masked in place, as in the reference.  Returns
+ * S2DWC_ERROR_ARTH_WARNING (outputs written) when a scale has zero variance
+ * and S2DWC_ERROR_SIZE_INVALID when one has fewer than two unmasked samples,
+ * the reference's two error cases. */
+int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double alpha, double *mean,
+                       double *var, double *skew, double *kur, const double *const *mask_scales,
+                       double *five, double *six);
 
 /* Synchronises with the device and reports S2DWC_ERROR_CUDA if a split-form
  * kernel gave up waiting on its tensor-core pipeline (each wait is bounded

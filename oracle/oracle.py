@@ -225,3 +225,25 @@ def test_gen_flm(L, seed=1):
     flm = np.zeros((L + 1, L + 1), dtype=np.complex128, order="F")
     lib().orc_test_gen_flm(int(L), _p(flm), int(seed))
     return flm
+
+
+def stat_moments(wavdyn, J, B, N, alpha, mask=None, higher=True):
+    """s2dw_stat_moments on copies of the per-scale arrays: returns (status,
+    moments) with moments a (J+1, 6) array of mean, var, skew, kur, five, six
+    (five and six zero when higher is False) and the masked coefficients
+    (the reference masks wavdyn in place)."""
+    ws = [np.array(w, dtype=np.float64, order="F", copy=True) for w in wavdyn]
+    ptrs = (_dp * (J + 1))(*[_p(w) for w in ws])
+    mk = None
+    if mask is not None:
+        ms = [np.asfortranarray(m, dtype=np.float64) for m in mask]
+        mk = (_dp * (J + 1))(*[_p(m) for m in ms])
+    out = np.zeros((6, J + 1))
+    L = lib()
+    L.orc_stat_moments.restype = ctypes.c_int
+    L.orc_stat_moments.argtypes = [ctypes.POINTER(_dp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                   _dp, _dp, _dp, _dp, ctypes.POINTER(_dp), _dp, _dp]
+    rows = [out[i].ctypes.data_as(_dp) for i in range(6)]
+    st = L.orc_stat_moments(ptrs, J, B, N, float(alpha), rows[0], rows[1], rows[2], rows[3], mk,
+                            rows[4] if higher else None, rows[5] if higher else None)
+    return st, out.T.copy(), ws

@@ -862,3 +862,80 @@ void orc_set_num_threads(int n)
     (void)n;
 #endif
 }
+
+/* ------------------------------------------------------------------------
+ * s2dw_stat_moments (src/mod/s2dw_stat_mod.f90:81-275), per scale jj:
+ * band limits as :108-118; optional mask applied to the coefficients in
+ * place (:121-125) and nj = nint(sum(mask)) (:128-132); nj < 2 is an error
+ * (:133-136); mean and the sums of powers 1..6 of s = w - mean over the
+ * samples with |mask - 1| < TOL_ZERO (all samples without a mask), summed in
+ * array order like Fortran's sum (:147-195, :199-242); variance with the n-1
+ * correction (:196, :244); zero variance (< TOL_ZERO) sets the higher moments
+ * to zero and raises the ARTH_WARNING code (:248-257); otherwise the
+ * standardisations of :259-268.  five / six may be NULL (optional).
+ * Returns 0, S2DW_ERROR_ARTH_WARNING (6) or S2DW_ERROR_SIZE_INVALID (8).
+ * ------------------------------------------------------------------------ */
+int orc_stat_moments(double *const *wav, int J, int B, int N, double alpha, double *mean, double *var,
+                     double *skew, double *kur, const double *const *mask, double *five, double *six)
+{
+    const double TOL_ZERO = 1e-12;
+    int status = 0;
+    for (int jj = 0; jj <= J; jj++) {
+        int hi, lo;
+        orc_band_limits(jj, B, alpha, &hi, &lo);
+        const long long n = (long long)(2 * hi - 1) * (2 * hi) * N;
+        double *w = wav[jj];
+        const double *mk = mask ? mask[jj] : NULL;
+        long long nj;
+        if (mk) {
+            double sm = 0.0;
+            for (long long i = 0; i < n; i++) w[i] *= mk[i];
+            for (long long i = 0; i < n; i++) sm += mk[i];
+            nj = (long long)llround(sm);
+        } else {
+            nj = n;
+        }
+        if (nj < 2) return 8;
+        double m = 0.0;
+        for (long long i = 0; i < n; i++)
+            if (!mk || fabs(mk[i] - 1.0) < TOL_ZERO) m += w[i];
+        m /= (double)nj;
+        double ep = 0.0, p2 = 0.0, p3 = 0.0, p4 = 0.0, p5 = 0.0, p6 = 0.0;
+        for (long long i = 0; i < n; i++) {
+            if (mk && !(fabs(mk[i] - 1.0) < TOL_ZERO)) continue;
+            const double s = w[i] - m;
+            double p = s * s;
+            ep += s;
+            p2 += p;
+            p *= s;
+            p3 += p;
+            p *= s;
+            p4 += p;
+            p *= s;
+            p5 += p;
+            p *= s;
+            p6 += p;
+        }
+        const double v = (p2 - ep * ep / (double)nj) / (double)(nj - 1);
+        const double sdev = sqrt(v);
+        mean[jj] = m;
+        var[jj] = v;
+        if (v < TOL_ZERO) {
+            status = 6;
+            skew[jj] = 0.0;
+            kur[jj] = 0.0;
+            if (five) {
+                five[jj] = 0.0;
+                if (six) six[jj] = 0.0;
+            }
+        } else {
+            skew[jj] = p3 / ((double)nj * sdev * sdev * sdev);
+            kur[jj] = p4 / ((double)nj * v * v) - 3.0;
+            if (five) {
+                five[jj] = p5 / ((double)nj * sdev * sdev * sdev * sdev * sdev);
+                if (six) six[jj] = p6 / ((double)nj * v * v * v) - 15.0;
+            }
+        }
+    }
+    return status;
+}

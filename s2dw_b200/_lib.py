@@ -44,6 +44,9 @@ SIGNATURES = {
     "s2dwc_plan_analysis_batch": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_synthesis_batch": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "s2dwc_plan_check": (_i, [_vp]),
+    "s2dwc_plan_stat_moments": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "s2dwc_stat_moments": (_i, [ctypes.POINTER(_dp), _i, _i, _i, _d, _dp, _dp, _dp, _dp, ctypes.POINTER(_dp),
+                                _dp, _dp]),
     "s2dwc_plan_launch_count": (_i, [_vp, _ip, _ip]),
     "s2dwc_plan_set_timing": (_i, [_vp, _i]),
     "s2dwc_plan_timing": (_i, [_vp, _i, _llp, _dp]),

@@ -166,3 +166,34 @@ def s2dw_core_free_wavdyn(wavdyn):
     """s2dw_core_free_wavdyn (s2dw_core_mod.f90:1289)."""
     if isinstance(wavdyn, list):
         wavdyn.clear()
+
+
+def s2dw_stat_moments(wavdyn, J, B, N, alpha, wavdyn_mask=None, higher=True):
+    """s2dw_stat_moments (src/mod/s2dw_stat_mod.f90:81-275) through
+    s2dwc_stat_moments: returns (mean, var, skew, kur, five, six) arrays of
+    J+1 values (five and six None when `higher` is False) and the status, 0 or
+    S2DW_ERROR_ARTH_WARNING (6, a scale with zero variance: its higher
+    moments are zero).  With a mask the coefficient arrays are masked in
+    place, as in the reference (they must then be float64 Fortran-order
+    arrays).  Fewer than two unmasked samples raises S2DWError (code 8)."""
+    ws = []
+    for j in range(J + 1):
+        w = wavdyn[j]
+        if wavdyn_mask is not None and not (isinstance(w, np.ndarray) and w.dtype == np.float64
+                                            and w.flags.f_contiguous):
+            raise ValueError("with a mask, wavdyn arrays are masked in place: pass float64 Fortran-order arrays")
+        ws.append(_f64(w, wav_scale_shape(j, B, N, alpha)))
+    ptrs = (_dp * (J + 1))(*[_p(w) for w in ws])
+    mk = None
+    if wavdyn_mask is not None:
+        ms = [_f64(m, wav_scale_shape(j, B, N, alpha)) for j, m in enumerate(wavdyn_mask)]
+        mk = (_dp * (J + 1))(*[_p(m) for m in ms])
+    out = [np.zeros(J + 1) for _ in range(6)]
+    st = lib().s2dwc_stat_moments(ptrs, int(J), int(B), int(N), float(alpha), _p(out[0]), _p(out[1]), _p(out[2]),
+                                  _p(out[3]), mk, _p(out[4]) if higher else None,
+                                  _p(out[5]) if higher else None)
+    if st not in (0, 6):
+        check(st)
+    if not higher:
+        out[4] = out[5] = None
+    return tuple(out), st

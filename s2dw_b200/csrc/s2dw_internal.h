@@ -263,6 +263,23 @@ int launch_split_dexp(const SplitArgs &a, cudaStream_t s);
 int launch_split_fdig(const FdigArgs &a, cudaStream_t s);
 int launch_split(const SplitArgs &a, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Moments of the wavelet coefficients per scale (s2dw_stats.cu)
+// ---------------------------------------------------------------------------
+constexpr int STAT_P = 64;  // blocks per (map, scale) in the reduction passes
+struct StatArgs {
+    int J, nmaps;
+    long long wtot;            // doubles per map in the packed layout
+    long long off[17];         // scale offsets (J+2 entries)
+    const double *wav;         // map k at wav + k*wtot
+    const double *mask;        // packed layout of one map, or null
+    double *part;              // nmaps*(J+1)*STAT_P*6 partial sums
+    double *mean_nj;           // nmaps*(J+1)*2
+    double *out;               // nmaps*(J+1)*6: mean, var, skew, kur, five, six
+    int *flags;                // nmaps*(J+1): 1 zero variance, 2 fewer than two samples
+};
+int launch_stat_moments(const StatArgs &a, cudaStream_t s);
+
 // Address on `device` (which must be current) of the static scratch array of
 // s2dwc_plan_analysis_noalloc, looked up once per device.
 int noalloc_scratch(int device, void **ptr);

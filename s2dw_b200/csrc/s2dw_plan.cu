@@ -91,6 +91,9 @@ struct s2dwc_plan {
     double2 *sp_V2f = nullptr, *sp_part = nullptr;
     long long sp_pstride = 0;
     int *sp_err = nullptr;
+    // moments of the coefficients (built on first use): 32 maps per pass
+    double *st_part = nullptr, *st_mean = nullptr;
+    int *st_flags = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
 
@@ -1246,6 +1249,114 @@ int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const do
         if (st) return st;
     }
     return S2DWC_OK;
+}
+
+int s2dwc_plan_stat_moments(s2dwc_plan *p, int nmaps, const double *d_wav, const double *d_mask, double *d_moments,
+                            void *stream)
+{
+    if (!p || !d_wav || !d_moments) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_stat_moments: null pointer");
+    if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_stat_moments: nmaps=%d", nmaps);
+    DeviceGuard dg(p->device);
+    constexpr int G = 32;
+    int st;
+    if (!p->st_part) {
+        const size_t ny = (size_t)G * (p->J + 1);
+        if ((st = dev_alloc(p, &p->st_part, ny * STAT_P * 6)) || (st = dev_alloc(p, &p->st_mean, ny * 2)) ||
+            (st = dev_alloc(p, &p->st_flags, ny)))
+            return st;
+    }
+    const long long wtot = p->wav_off[p->J + 1];
+    for (int g0 = 0; g0 < nmaps; g0 += G) {
+        StatArgs a{};
+        a.J = p->J;
+        a.nmaps = std::min(G, nmaps - g0);
+        a.wtot = wtot;
+        for (int j = 0; j <= p->J + 1; j++) a.off[j] = p->wav_off[j];
+        a.wav = d_wav + (size_t)g0 * wtot;
+        a.mask = d_mask;
+        a.part = p->st_part;
+        a.mean_nj = p->st_mean;
+        a.out = d_moments + (size_t)g0 * (p->J + 1) * 6;
+        a.flags = p->st_flags;
+        if ((st = launch_stat_moments(a, (cudaStream_t)stream))) return st;
+    }
+    return S2DWC_OK;
+}
+
+int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double alpha, double *mean, double *var,
+                       double *skew, double *kur, const double *const *mask_scales, double *five, double *six)
+{
+    if (!wav_scales || !mean || !var || !skew || !kur)
+        return set_error(S2DWC_ERROR_ARG_INVALID, "stat_moments: null pointer");
+    if (B < 2 || N < 1 || J < 0 || J > 15 || !(alpha > 1.0))
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "stat_moments: B=%d N=%d J=%d alpha=%g", B, N, J, alpha);
+    for (int j = 0; j <= J; j++)
+        if (!wav_scales[j] || (mask_scales && !mask_scales[j]))
+            return set_error(S2DWC_ERROR_ARG_INVALID, "stat_moments: scale %d is null", j);
+    StatArgs a{};
+    a.J = J;
+    a.nmaps = 1;
+    a.off[0] = 0;
+    for (int j = 0; j <= J; j++) {
+        int hi, lo;
+        band_limits(j, B, alpha, &hi, &lo);
+        a.off[j + 1] = a.off[j] + (long long)(2 * hi - 1) * (2 * hi) * N;
+    }
+    a.wtot = a.off[J + 1];
+    const size_t ny = (size_t)J + 1;
+    // one device block for everything this call needs, freed before return
+    const size_t nw = (size_t)a.wtot, nm = mask_scales ? nw : 0;
+    const size_t bytes = 8 * (nw + nm + ny * STAT_P * 6 + ny * 2 + ny * 6) + 4 * ny + 256;
+    char *blk = nullptr;
+    cudaError_t e = cudaMalloc(&blk, bytes);
+    if (e != cudaSuccess)
+        return set_error(S2DWC_ERROR_MEM_ALLOC_FAIL, "stat_moments: cudaMalloc of %zu bytes failed: %s", bytes,
+                         cudaGetErrorString(e));
+    std::unique_ptr<char, void (*)(char *)> guard(blk, [](char *q) { cudaFree(q); });
+    double *dw = reinterpret_cast<double *>(blk), *dm = dw + nw, *dpart = dm + nm, *dmean = dpart + ny * STAT_P * 6,
+           *dout = dmean + ny * 2;
+    int *dflags = reinterpret_cast<int *>(dout + ny * 6);
+    for (int j = 0; j <= J; j++) {
+        const size_t n = (size_t)(a.off[j + 1] - a.off[j]);
+        S2DW_CUDA_TRY(cudaMemcpy(dw + a.off[j], wav_scales[j], 8 * n, cudaMemcpyHostToDevice));
+        if (mask_scales) S2DW_CUDA_TRY(cudaMemcpy(dm + a.off[j], mask_scales[j], 8 * n, cudaMemcpyHostToDevice));
+    }
+    a.wav = dw;
+    a.mask = mask_scales ? dm : nullptr;
+    a.part = dpart;
+    a.mean_nj = dmean;
+    a.out = dout;
+    a.flags = dflags;
+    int st = launch_stat_moments(a, 0);
+    if (st) return st;
+    std::vector<double> out(ny * 6);
+    std::vector<int> flags(ny);
+    S2DW_CUDA_TRY(cudaMemcpy(out.data(), dout, 8 * out.size(), cudaMemcpyDeviceToHost));
+    S2DW_CUDA_TRY(cudaMemcpy(flags.data(), dflags, 4 * flags.size(), cudaMemcpyDeviceToHost));
+    // the reference masks its input in place (s2dw_stat_mod.f90:121-125)
+    if (mask_scales)
+        for (int j = 0; j <= J; j++) {
+            const long long n = a.off[j + 1] - a.off[j];
+            double *w = wav_scales[j];
+            const double *m = mask_scales[j];
+#pragma omp parallel for
+            for (long long i = 0; i < n; i++) w[i] *= m[i];
+        }
+    int status = S2DWC_OK;
+    for (int j = 0; j <= J; j++) {
+        if (flags[j] == 2)
+            return set_error(S2DWC_ERROR_SIZE_INVALID, "stat_moments: scale %d has fewer than two samples", j);
+        mean[j] = out[6 * j];
+        var[j] = out[6 * j + 1];
+        skew[j] = out[6 * j + 2];
+        kur[j] = out[6 * j + 3];
+        if (five) five[j] = out[6 * j + 4];
+        if (five && six) six[j] = out[6 * j + 5];
+        if (flags[j] == 1)
+            status = set_error(S2DWC_ERROR_ARTH_WARNING,
+                               "stat_moments: scale %d has zero variance; its higher moments are set to zero", j);
+    }
+    return status;
 }
 
 int s2dwc_plan_check(s2dwc_plan *p)

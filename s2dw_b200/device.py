@@ -146,6 +146,17 @@ class Plan:
                                                self._ptr(scoeff, torch.complex128, n * self.bl_scoeff ** 2),
                                                self._stream(stream)))
 
+    def stat_moments(self, wav, moments, mask=None, stream=None):
+        """Moments per scale of wav.shape[0] device maps (packed layout) into
+        moments (n, J+1, 6): mean, var, skew, kur, five, six."""
+        import torch
+
+        n = int(wav.shape[0]) if wav.dim() > 1 else 1
+        check(lib().s2dwc_plan_stat_moments(self._h, n, self._ptr(wav, torch.float64, n * self.wav_size),
+                                            self._ptr(mask, torch.float64, self.wav_size),
+                                            self._ptr(moments, torch.float64, n * (self.J + 1) * 6),
+                                            self._stream(stream)))
+
     def check(self):
         """Raises S2DWError if a split-form kernel gave up waiting (synchronises)."""
         check(lib().s2dwc_plan_check(self._h))

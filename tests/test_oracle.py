@@ -147,3 +147,61 @@ def test_linearity():
     w3, _ = O.analysis_dynamic(np.asfortranarray(2 * f1 - f2), K, S, J, B, N, bs, alpha)
     for a, b, c in zip(w1, w2, w3):
         np.testing.assert_allclose(c, 2 * a - b, atol=1e-13)
+
+
+def _np_moments(ws, masks=None):
+    """Straight numpy statement of s2dw_stat_moments' formulas."""
+    out, status = [], 0
+    for j, w in enumerate(ws):
+        x = np.asarray(w, dtype=np.float64).ravel(order="F")
+        if masks is not None:
+            m = np.asarray(masks[j]).ravel(order="F")
+            nj = int(round(m.sum()))
+            x = (x * m)[np.abs(m - 1.0) < 1e-12]
+        else:
+            nj = x.size
+        mu = x.sum() / nj
+        s = x - mu
+        v = ((s ** 2).sum() - s.sum() ** 2 / nj) / (nj - 1)
+        if v < 1e-12:
+            status = 6
+            out.append([mu, v, 0, 0, 0, 0])
+        else:
+            sd = np.sqrt(v)
+            out.append([mu, v, (s ** 3).sum() / (nj * sd ** 3), (s ** 4).sum() / (nj * v * v) - 3,
+                        (s ** 5).sum() / (nj * sd ** 5), (s ** 6).sum() / (nj * v ** 3) - 15])
+    return np.array(out), status
+
+
+def test_oracle_stat_moments_match_numpy():
+    from s2dw_b200 import core
+
+    B, N, alpha = 16, 3, 2.0
+    J = core.s2dw_core_comp_Jmax(B, alpha)
+    rng = np.random.default_rng(4)
+    ws = [np.asfortranarray(rng.standard_normal(core.wav_scale_shape(j, B, N, alpha)) ** 3 + 0.1)
+          for j in range(J + 1)]
+    st, m, _ = O.stat_moments(ws, J, B, N, alpha)
+    ref, st_ref = _np_moments(ws)
+    assert st == st_ref == 0
+    np.testing.assert_allclose(m, ref, rtol=1e-10, atol=1e-12)
+    masks = [np.asfortranarray((rng.random(w.shape) < 0.7).astype(np.float64)) for w in ws]
+    st, m, masked = O.stat_moments(ws, J, B, N, alpha, mask=masks)
+    ref, _ = _np_moments(ws, masks)
+    np.testing.assert_allclose(m, ref, rtol=1e-10, atol=1e-12)
+    for w, mk, wm in zip(ws, masks, masked):
+        np.testing.assert_array_equal(wm, w * mk)  # masked in place, as the reference
+
+
+def test_oracle_stat_moments_zero_variance_and_too_few_samples():
+    from s2dw_b200 import core
+
+    B, N, alpha = 8, 2, 2.0
+    J = core.s2dw_core_comp_Jmax(B, alpha)
+    ws = [np.full(core.wav_scale_shape(j, B, N, alpha), 0.25, order="F") for j in range(J + 1)]
+    st, m, _ = O.stat_moments(ws, J, B, N, alpha)
+    assert st == 6 and np.all(m[:, 2:] == 0) and np.allclose(m[:, 0], 0.25)
+    masks = [np.zeros(w.shape, order="F") for w in ws]
+    masks[0].flat[0] = 1.0
+    st, _, _ = O.stat_moments(ws, J, B, N, alpha, mask=masks)
+    assert st == 8
