@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=4096,
                     help="mixed request stream for the serving p50/p99 (0 = skip)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of replaying a CUDA graph")
+    ap.add_argument("--no-large", action="store_true", help="skip the B=2048 N=8 single-transform section")
     ap.add_argument("--split-maps", type=int, default=32,
                     help="maps per batch for the split-precision measurement (0: skip)")
     return ap.parse_args()
@@ -253,6 +254,52 @@ def split_stats(B, N, alpha, J, maps, repeats=3):
             "max_w_err": werr, "max_flm_err_synthesis": synerr, "recon_err": recon,
             "form": "split analysis and synthesis contractions (tcgen05 int8 digits, 6 bytes, 28 exact products); FP64 recurrences, tables and FFTs",
             "workload": f"B={B} N={N} alpha={alpha:g} J={J}, {maps} seeded maps per batch, device-resident"}
+
+
+def large_stats(B=2048, N=8, alpha=2.0, power=1.2, steps=6, warmup=2):
+    """The large single transform: B=2048, N=8, alpha=2, J=Jmax, one map with
+    C_l = (1/(l(l+1)))^1.2, FP64 form: device time per analysis+synthesis
+    pair (scales on the plan's streams), reconstruction error, and the
+    serialised time of each kernel kind."""
+    import torch
+
+    from s2dw_b200.core import s2dw_core_comp_Jmax
+    from s2dw_b200.device import Plan
+    from s2dw_b200.workload import gaussian_flm, transform_setup
+
+    J = s2dw_core_comp_Jmax(B, alpha)
+    t = transform_setup(B, N, alpha, J)
+    plan = Plan(B, N, alpha, J)
+    plan.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    flm = gaussian_flm(B, seed=0, power=power)
+    d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
+    d_wav = torch.empty(plan.wav_size, dtype=torch.float64, device="cuda")
+    d_sc = torch.empty(max(1, t["bl_scoeff"] ** 2), dtype=torch.complex128, device="cuda")
+    d_out = torch.empty_like(d_flm)
+    for _ in range(warmup):
+        plan.analysis(d_flm, d_wav, d_sc)
+        plan.synthesis(d_wav, d_sc, d_out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        plan.analysis(d_flm, d_wav, d_sc)
+        plan.synthesis(d_wav, d_sc, d_out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    recon = float(np.abs(d_out.cpu().numpy().T - flm).max() / np.abs(flm).max())
+    plan.set_timing(True)
+    plan.timing(reset=True)
+    plan.analysis(d_flm, d_wav, d_sc)
+    plan.synthesis(d_wav, d_sc, d_out)
+    torch.cuda.synchronize()
+    kt = plan.timing(reset=True)
+    plan.close()
+    return {"workload": f"B={B} N={N} alpha={alpha:g} J={J}, one map, C_l=(1/(l(l+1)))^{power}, FP64 form",
+            "value": 1e3 / ms, "unit": "pairs/s", "ms_per_pair": ms, "recon_err_rel_max_flm": recon,
+            "wav_bytes": 8 * plan.wav_size, "steps": steps,
+            "kernels_ms": {k: v[1] for k, v in kt.items() if v[0]}}
 
 
 def fft_flops_per_pair(B, N, alpha, J):
@@ -526,6 +573,13 @@ def main():
         except Exception as ex:
             serving = {"error": str(ex)[:300]}
 
+    large = None
+    if not args.no_large and rank == 0:
+        try:
+            large = large_stats()
+        except Exception as ex:
+            large = {"error": str(ex)[:300]}
+
     split = None
     if args.split_maps > 0:
         try:
@@ -553,7 +607,7 @@ def main():
                        "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
                        "recon_err": recon},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
-            "split": split,
+            "split": split, "large": large,
             "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
         }
         print(json.dumps(line), flush=True)
