@@ -1038,7 +1038,10 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
     double2 *ph = twl + 64;
     const int t = threadIdx.x;
     const int bl = a.bl, n = 2 * bl - 1, N = a.N, Bout = a.czt.spec.Bout;
-    const int g = blockIdx.y, rr = blockIdx.x;  // row = (g or q, m or b pair)
+    // row = (g or q, m or b pair); the synthesis beta modes put q on the fast
+    // grid axis so that the CTAs of one m, which read the same N rows of V,
+    // run together and the repeated reads hit L2
+    const int g = SYNB ? blockIdx.x : blockIdx.y, rr = SYNB ? blockIdx.y : blockIdx.x;
     const double2 zero = make_double2(0.0, 0.0);
 
     for (int i = t; i < M / 64; i += THREADS) twh[i] = a.tw.hi[i];
@@ -1406,7 +1409,8 @@ static int launch_large_t(const CztArgs &a, cudaStream_t s)
     }
     // rows are (g or q) x (m or b pair); every mode has bl rows per g
     const int ng = a.rows / a.bl;
-    dim3 grid(a.bl, ng);
+    constexpr bool synb = (MODE == CZT_SYN_BETA || MODE == FFT_SYN_BETA);
+    const dim3 grid = synb ? dim3(ng, a.bl) : dim3(a.bl, ng);
     fft_large_kernel<MODE, LGM><<<grid, M / 16, smem, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
