@@ -297,15 +297,29 @@ __device__ __forceinline__ void mma_commit(uint32_t bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t *r)
+// The seven level accumulators of 16 columns: seven loads, one wait.
+__device__ __forceinline__ void tmem_ld16x7(uint32_t taddr, int32_t (&r)[7][16])
 {
+    static_assert(LEV == 7 && COLS == 64, "level layout");
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%112];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%113];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47}, [%114];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%115];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%64, %65, %66, %67, %68, %69, %70, %71, %72, %73, %74, %75, %76, %77, %78, %79}, [%116];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%80, %81, %82, %83, %84, %85, %86, %87, %88, %89, %90, %91, %92, %93, %94, %95}, [%117];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%96, %97, %98, %99, %100, %101, %102, %103, %104, %105, %106, %107, %108, %109, %110, %111}, [%118];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[0][2]), "=r"(r[0][3]), "=r"(r[0][4]), "=r"(r[0][5]), "=r"(r[0][6]), "=r"(r[0][7]), "=r"(r[0][8]), "=r"(r[0][9]), "=r"(r[0][10]), "=r"(r[0][11]), "=r"(r[0][12]), "=r"(r[0][13]), "=r"(r[0][14]), "=r"(r[0][15]),
+          "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[1][2]), "=r"(r[1][3]), "=r"(r[1][4]), "=r"(r[1][5]), "=r"(r[1][6]), "=r"(r[1][7]), "=r"(r[1][8]), "=r"(r[1][9]), "=r"(r[1][10]), "=r"(r[1][11]), "=r"(r[1][12]), "=r"(r[1][13]), "=r"(r[1][14]), "=r"(r[1][15]),
+          "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[2][2]), "=r"(r[2][3]), "=r"(r[2][4]), "=r"(r[2][5]), "=r"(r[2][6]), "=r"(r[2][7]), "=r"(r[2][8]), "=r"(r[2][9]), "=r"(r[2][10]), "=r"(r[2][11]), "=r"(r[2][12]), "=r"(r[2][13]), "=r"(r[2][14]), "=r"(r[2][15]),
+          "=r"(r[3][0]), "=r"(r[3][1]), "=r"(r[3][2]), "=r"(r[3][3]), "=r"(r[3][4]), "=r"(r[3][5]), "=r"(r[3][6]), "=r"(r[3][7]), "=r"(r[3][8]), "=r"(r[3][9]), "=r"(r[3][10]), "=r"(r[3][11]), "=r"(r[3][12]), "=r"(r[3][13]), "=r"(r[3][14]), "=r"(r[3][15]),
+          "=r"(r[4][0]), "=r"(r[4][1]), "=r"(r[4][2]), "=r"(r[4][3]), "=r"(r[4][4]), "=r"(r[4][5]), "=r"(r[4][6]), "=r"(r[4][7]), "=r"(r[4][8]), "=r"(r[4][9]), "=r"(r[4][10]), "=r"(r[4][11]), "=r"(r[4][12]), "=r"(r[4][13]), "=r"(r[4][14]), "=r"(r[4][15]),
+          "=r"(r[5][0]), "=r"(r[5][1]), "=r"(r[5][2]), "=r"(r[5][3]), "=r"(r[5][4]), "=r"(r[5][5]), "=r"(r[5][6]), "=r"(r[5][7]), "=r"(r[5][8]), "=r"(r[5][9]), "=r"(r[5][10]), "=r"(r[5][11]), "=r"(r[5][12]), "=r"(r[5][13]), "=r"(r[5][14]), "=r"(r[5][15]),
+          "=r"(r[6][0]), "=r"(r[6][1]), "=r"(r[6][2]), "=r"(r[6][3]), "=r"(r[6][4]), "=r"(r[6][5]), "=r"(r[6][6]), "=r"(r[6][7]), "=r"(r[6][8]), "=r"(r[6][9]), "=r"(r[6][10]), "=r"(r[6][11]), "=r"(r[6][12]), "=r"(r[6][13]), "=r"(r[6][14]), "=r"(r[6][15])
+        : "r"(taddr), "r"(taddr + 64), "r"(taddr + 128), "r"(taddr + 192), "r"(taddr + 256), "r"(taddr + 320),
+          "r"(taddr + 384)
+        : "memory");
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -702,13 +716,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
 #pragma unroll
             for (int i = 0; i < 16; i++) acc[i] = 0.0;
             if (nout > 0 && !abort) {
+                int32_t r[LEV][16];
+                tmem_ld16x7(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + col0, r);
 #pragma unroll
                 for (int lev = 0; lev < LEV; lev++) {
-                    int32_t r[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + lev * COLS + col0, r);
                     const double wgt = pow2i(-8 * lev);
 #pragma unroll
-                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
+                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[lev][i], wgt, acc[i]);
                 }
             }
 #pragma unroll
@@ -1071,13 +1085,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArg
 #pragma unroll
             for (int i = 0; i < 16; i++) acc[i] = 0.0;
             if (!abort) {
+                int32_t r[LEV][16];
+                tmem_ld16x7(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + col0, r);
 #pragma unroll
                 for (int lev = 0; lev < LEV; lev++) {
-                    int32_t r[16];
-                    tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + lev * COLS + col0, r);
                     const double wgt = pow2i(-8 * lev);
 #pragma unroll
-                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[i], wgt, acc[i]);
+                    for (int i = 0; i < 16; i++) acc[i] = fma((double)r[lev][i], wgt, acc[i]);
                 }
             }
             if (valid) {
