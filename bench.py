@@ -56,6 +56,9 @@ def parse():
                     help="mixed request stream for the serving p50/p99 (0 = skip)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly instead of replaying a CUDA graph")
     ap.add_argument("--no-large", action="store_true", help="skip the B=2048 N=8 single-transform section")
+    ap.add_argument("--large-split-maps", type=int, default=8,
+                    help="maps per split-form batch in the B=2048 N=8 section (0: skip)")
+    ap.add_argument("--no-b256", action="store_true", help="skip the B=256 N=5 split-vs-FP64 section")
     ap.add_argument("--split-maps", type=int, default=32,
                     help="maps per batch for the split-precision measurement (0: skip)")
     return ap.parse_args()
@@ -137,17 +140,10 @@ def contraction_flops_per_scale(B, N, alpha, J):
     return ana, syn
 
 
-def serving_stats(n_requests, device):
-    """The mixed serving stream: Poisson arrivals, B uniform over
-    {32,...,1024}, N uniform over 1..8, alpha in {2,3}, J=Jmax, half analyses
-    and half syntheses (inputs from analyses of seeded maps).  The arrival
-    rate is 70% of the throughput measured with every request arriving at
-    once, so that queues stay finite and the percentiles reflect overlap."""
-    from s2dw_b200.serving import Server, make_stream
-
-    reqs, inputs = make_stream(n_requests, seed=2026, rate_hz=1e9)
-    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device)
-    # warm the plan/graph cache with one request per (config, kind)
+def _serve(srv, reqs, rate=None):
+    """Warm-up (one request per configuration and kind), then the whole
+    stream at once (saturation throughput), then Poisson arrivals at `rate`
+    (default 70% of the saturation throughput) for the latency percentiles."""
     seen, warm = set(), []
     for r in reqs:
         k = (r.B, r.N, r.alpha, r.J, r.kind)
@@ -160,29 +156,60 @@ def serving_stats(n_requests, device):
     for r in reqs:
         r.arrival = 0.0
     cap = srv.run(reqs)["throughput_rps"]
-    rate = 0.7 * cap
+    rate = 0.7 * cap if rate is None else rate
     rng = np.random.default_rng(7)
     t = 0.0
     for r in reqs:
         t += rng.exponential(1.0 / rate)
         r.arrival = t
     st = srv.run(reqs)
-    srv.close()
-    del inputs
-    st.update({"offered_rate_rps": rate, "saturation_rps": cap, "form": "fp64",
-               "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
-                         "half analysis / half synthesis, device-resident inputs, graph replay"})
+    st.update({"offered_rate_rps": rate, "saturation_rps": cap})
     return st
 
 
-def split_stats(B, N, alpha, J, maps, repeats=3):
+def serving_stats(n_requests, device, split=True):
+    """The mixed serving stream: Poisson arrivals, B uniform over
+    {32,...,1024}, N uniform over 1..8, alpha in {2,3}, J=Jmax, half analyses
+    and half syntheses (inputs from analyses of seeded maps).  The arrival
+    rate is 70% of the FP64 server's throughput with every request arriving
+    at once, so that queues stay finite and the percentiles reflect overlap.
+    The split-precision server then serves the same stream at the same
+    offered rate, batching the waiting requests of a configuration and kind
+    (up to 1 GB of packed wavelets per batch)."""
+    from s2dw_b200.serving import Server, make_stream
+
+    reqs, inputs = make_stream(n_requests, seed=2026, rate_hz=1e9)
+    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device)
+    st = _serve(srv, reqs)
+    srv.close()
+    st.update({"form": "fp64",
+               "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
+                         "half analysis / half synthesis, device-resident inputs, graph replay"})
+    if split:
+        try:
+            srv = Server(hbm_budget_bytes=80 << 30, slots_per_config=2, use_graphs=True, device=device,
+                         form="split", batch_bytes=1 << 30)
+            sp = _serve(srv, reqs, rate=st["offered_rate_rps"])
+            srv.close()
+            sp["note"] = ("split-precision slots: waiting requests of one configuration and kind run as one "
+                          "tensor-core batch; same stream and offered rate as the FP64 server")
+            st["split"] = sp
+        except Exception as ex:  # reported, not fatal to the bench line
+            st["split"] = {"error": str(ex)[:300]}
+    del inputs
+    return st
+
+
+def split_stats(B, N, alpha, J, maps, repeats=3, power=1.0):
     """Split-precision form on a batch of `maps` seeded maps (the form's
     tensor-core contractions share their d-operand across the batch): device
     time of batched analysis+synthesis pairs per map for the split plan and for
     the FP64 plan on the same batch, the serialised contraction times of each
-    form, the split form's worst per-scale max|w_split - w_fp64| / max|w_fp64|,
-    its synthesis error max|flm_split - flm_fp64| / max|flm_fp64| on the same
-    coefficients, and the split pair's reconstruction error."""
+    form, the split form's max|w_split - w_fp64| / max|w_fp64| per scale (worst
+    map) and overall, its synthesis error max|flm_split - flm_fp64| /
+    max|flm_fp64| on the same coefficients, and the split pair's
+    reconstruction error (absolute and relative to max|flm|).  Errors are
+    reduced on the device."""
     import torch
 
     from s2dw_b200.device import Plan
@@ -193,8 +220,9 @@ def split_stats(B, N, alpha, J, maps, repeats=3):
     split = Plan(B, N, alpha, J, form=Plan.SPLIT)
     for p in (plain, split):
         p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
-    flms = [gaussian_flm(B, seed=k) for k in range(maps)]
+    flms = [gaussian_flm(B, seed=k, power=power) for k in range(maps)]
     d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
+    del flms
     bs2 = max(1, t["bl_scoeff"] ** 2)
     w_ref = torch.empty((maps, plain.wav_size), dtype=torch.float64, device="cuda")
     w_sp = torch.empty_like(w_ref)
@@ -208,19 +236,22 @@ def split_stats(B, N, alpha, J, maps, repeats=3):
     split.check()
     plain.synthesis_batch(w_sp, s_sp, out_ref)
     torch.cuda.synchronize()
-    wr, ws = w_ref.cpu().numpy(), w_sp.cpu().numpy()
     offs = plain.wav_offsets
-    werr = 0.0
-    for k in range(maps):
-        for j in range(J + 1):
-            a_, b_ = wr[k, offs[j]:offs[j + 1]], ws[k, offs[j]:offs[j + 1]]
-            sc = np.abs(a_).max()
-            if sc > 0:
-                werr = max(werr, float(np.abs(a_ - b_).max() / sc))
-    recon = max(float(np.abs(out[k].cpu().numpy().T - flms[k]).max()) for k in range(maps))
-    fo, fr = out.cpu().numpy(), out_ref.cpu().numpy()
-    synerr = max(float(np.abs(fo[k] - fr[k]).max() / np.abs(fr[k]).max()) for k in range(maps))
-    del wr, ws, fo, fr
+    per_scale = []
+    for j in range(J + 1):
+        a_, b_ = w_ref[:, offs[j]:offs[j + 1]], w_sp[:, offs[j]:offs[j + 1]]
+        sc = a_.abs().amax(dim=1)
+        d = (a_ - b_).abs().amax(dim=1)
+        r = torch.where(sc > 0, d / sc.clamp_min(1e-300), torch.zeros_like(d))
+        per_scale.append(float(r.max()))
+    werr = max(per_scale)
+    fmax = d_flm.abs().amax(dim=(1, 2))
+    dev = (out - d_flm).abs().amax(dim=(1, 2))
+    recon = float(dev.max())
+    recon_rel = float((dev / fmax).max())
+    synerr = float(((out - out_ref).abs().amax(dim=(1, 2)) / out_ref.abs().amax(dim=(1, 2))).max())
+    del w_ref, s_ref, out_ref
+    torch.cuda.empty_cache()
 
     def timed(ana, syn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -251,9 +282,11 @@ def split_stats(B, N, alpha, J, maps, repeats=3):
     return {"maps_per_batch": maps, "value": maps / t_split, "unit": "pairs/s",
             "fp64_same_batch": maps / t_fp64, "speedup_vs_fp64": t_fp64 / t_split,
             "kernels": contraction,
-            "max_w_err": werr, "max_flm_err_synthesis": synerr, "recon_err": recon,
+            "max_w_err": werr, "max_w_err_per_scale": per_scale, "max_flm_err_synthesis": synerr,
+            "recon_err": recon, "recon_err_rel_max_flm": recon_rel,
             "form": "split analysis and synthesis contractions (tcgen05 int8 digits, 6 bytes, 28 exact products); FP64 recurrences, tables and FFTs",
-            "workload": f"B={B} N={N} alpha={alpha:g} J={J}, {maps} seeded maps per batch, device-resident"}
+            "workload": f"B={B} N={N} alpha={alpha:g} J={J}, {maps} seeded maps per batch"
+                        + (f", C_l=(1/(l(l+1)))^{power:g}" if power != 1.0 else "") + ", device-resident"}
 
 
 def large_stats(B=2048, N=8, alpha=2.0, power=1.2, steps=6, warmup=2):
@@ -579,6 +612,21 @@ def main():
             large = large_stats()
         except Exception as ex:
             large = {"error": str(ex)[:300]}
+        if args.large_split_maps > 0 and "error" not in large:
+            from s2dw_b200.core import s2dw_core_comp_Jmax
+            try:
+                large["split"] = split_stats(2048, 8, 2.0, s2dw_core_comp_Jmax(2048, 2.0), args.large_split_maps,
+                                             repeats=1, power=1.2)
+            except Exception as ex:
+                large["split"] = {"error": str(ex)[:300]}
+
+    split_b256 = None
+    if args.split_maps > 0 and not args.no_b256 and rank == 0:
+        from s2dw_b200.core import s2dw_core_comp_Jmax
+        try:
+            split_b256 = split_stats(256, 5, 2.0, s2dw_core_comp_Jmax(256, 2.0), args.split_maps)
+        except Exception as ex:
+            split_b256 = {"error": str(ex)[:300]}
 
     split = None
     if args.split_maps > 0:
@@ -607,7 +655,7 @@ def main():
                        "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
                        "recon_err": recon},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
-            "split": split, "large": large,
+            "split": split, "split_b256": split_b256, "large": large,
             "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
         }
         print(json.dumps(line), flush=True)

@@ -193,6 +193,15 @@ int s2dwc_plan_analysis_batch(s2dwc_plan *plan, int nmaps, double *d_wav, double
 int s2dwc_plan_synthesis_batch(s2dwc_plan *plan, int nmaps, double *d_flm, const double *d_wav,
                                const double *d_scoeff, void *stream);
 
+/* Sizes the split form's map workspaces for batches of up to nmaps maps
+ * (at most 32 are held; larger batches run in groups of 32).  The split
+ * entry points grow these workspaces on demand, which frees the smaller ones:
+ * a CUDA graph captured before a growth must not be replayed after it, and a
+ * growth inside a capture fails with S2DWC_ERROR_ARG_INVALID.  Call this
+ * before capturing batches.  Needs the kernel tables (s2dwc_plan_set_tables);
+ * no effect in the FP64 form.  Not in the reference. */
+int s2dwc_plan_reserve(s2dwc_plan *plan, int nmaps, void *stream);
+
 /* Moments of the wavelet coefficients per scale for `nmaps` device-resident
  * maps in the packed layout (map k at d_wav + k*offsets[J+1]): the
  * computation of s2dw_stat_moments (src/mod/s2dw_stat_mod.f90:81-275) without

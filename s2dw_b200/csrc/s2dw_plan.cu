@@ -76,7 +76,9 @@ struct s2dwc_plan {
         int snch = 0, sntiles = 0;
         int2 *stiles = nullptr;
         long long sexp_off = 0;
-        // per-scale workspaces (offsets in elements of the buffers below)
+        // per-scale workspaces (offsets in elements of the buffers below;
+        // tg_off and v2f_off count per map: the scale's region of a buffer
+        // that holds `sp_cap` maps starts at sp_cap * offset)
         long long fdig_off = 0, vdig_off = 0, fexp_off = 0, tg_off = 0, tb_off = 0, v2f_off = 0, vstride = 0;
     };
     std::vector<SplitScale> sp;
@@ -90,6 +92,10 @@ struct s2dwc_plan {
     uint8_t *sp_vdig = nullptr;
     double2 *sp_V2f = nullptr, *sp_part = nullptr;
     long long sp_pstride = 0;
+    // maps the map-proportional workspaces (Tg, V2f, part) hold: grown on
+    // demand up to the 32 maps of one tensor-core pass
+    int sp_cap = 0;
+    long long sp_tg_map = 0, sp_v2f_map = 0;
     int *sp_err = nullptr;
     // moments of the coefficients (built on first use): 32 maps per pass
     double *st_part = nullptr, *st_mean = nullptr;
@@ -129,6 +135,21 @@ int dev_alloc(s2dwc_plan *p, T **ptr, size_t count)
     p->ws_bytes += (long long)(count * sizeof(T));
     *ptr = static_cast<T *>(v);
     return S2DWC_OK;
+}
+
+// Frees a buffer of `count` elements allocated by dev_alloc.
+template <typename T>
+void dev_release(s2dwc_plan *p, T **ptr, size_t count)
+{
+    if (!*ptr) return;
+    for (size_t i = 0; i < p->allocs.size(); i++)
+        if (p->allocs[i] == static_cast<void *>(*ptr)) {
+            p->allocs.erase(p->allocs.begin() + (long)i);
+            break;
+        }
+    cudaFree(*ptr);
+    p->ws_bytes -= (long long)(std::max<size_t>(count, 1) * sizeof(T));
+    *ptr = nullptr;
 }
 
 template <typename T>
@@ -629,7 +650,7 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
 // Split form: per-scale workspaces (the scales of a batch run concurrently
 // on the plan's streams), tile lists and the per-row exponent tables (the
 // latter depend on the kernel tables and are rebuilt after set_tables).
-int split_prepare(s2dwc_plan *p, cudaStream_t s)
+int split_prepare(s2dwc_plan *p, int nmaps, cudaStream_t s)
 {
     int st;
     const int NP = p->NP, CH = split_chains(NP), MAPS = split_maps_per_pass(), MC = split_syn_mc(NP);
@@ -654,12 +675,12 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             S.fexp_off = fexp;
             fexp += (long long)bl * 64;
             S.tg_off = tg;
-            tg += (long long)MAPS * p->N * bl * bl;
+            tg += (long long)p->N * bl * bl;
             S.tb_off = tb;
             tb += (long long)p->N * bl * 2 * bl;
             S.vstride = (long long)NP * bl * Vs;
             S.v2f_off = v2f;
-            v2f += MAPS * S.vstride;
+            v2f += S.vstride;
             // analysis tiles (m, chain tile), longest walks (smallest first row) first
             std::vector<int2> tl;
             const int np = (bl + CH - 1) / CH;
@@ -686,10 +707,10 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
         if ((st = dev_alloc(p, &p->sp_dexp, (size_t)nd)) || (st = dev_alloc(p, &p->sp_sexp, (size_t)ns)) ||
             (st = dev_alloc(p, &p->sp_fexp, (size_t)fexp)) || (st = dev_alloc(p, &p->sp_vexp, (size_t)fexp)) ||
             (st = dev_alloc(p, &p->sp_fdig, (size_t)fdig)) || (st = dev_alloc(p, &p->sp_vdig, (size_t)vdig)) ||
-            (st = dev_alloc(p, &p->sp_Tg, (size_t)tg)) || (st = dev_alloc(p, &p->sp_Tb, (size_t)tb)) ||
-            (st = dev_alloc(p, &p->sp_V2f, (size_t)v2f)) ||
-            (st = dev_alloc(p, &p->sp_part, (size_t)MAPS * p->sp_pstride)) || (st = dev_alloc(p, &p->sp_err, 1)))
+            (st = dev_alloc(p, &p->sp_Tb, (size_t)tb)) || (st = dev_alloc(p, &p->sp_err, 1)))
             return st;
+        p->sp_tg_map = tg;
+        p->sp_v2f_map = v2f;
         S2DW_CUDA_TRY(cudaMemsetAsync(p->sp_err, 0, sizeof(int), s));
         // gamma-DFT phases exp(i pi n g / N), [g*16 + n+N-1]
         std::vector<double2> ph((size_t)p->N * 16, make_double2(0.0, 0.0));
@@ -700,6 +721,29 @@ int split_prepare(s2dwc_plan *p, cudaStream_t s)
             }
         if ((st = dev_upload(p, &p->sp_ph, ph))) return st;
         p->sp_alloc = true;
+    }
+    const int need = std::max(1, std::min(MAPS, nmaps));
+    if (need > p->sp_cap) {
+        // the buffers may still be read by earlier work of this plan
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        S2DW_CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return set_error(S2DWC_ERROR_ARG_INVALID,
+                             "split workspaces for %d maps must be sized before graph capture (run the batch once)",
+                             need);
+        if (p->sp_cap > 0) {
+            S2DW_CUDA_TRY(cudaStreamSynchronize(s));
+            for (auto st2 : p->streams) S2DW_CUDA_TRY(cudaStreamSynchronize(st2));
+        }
+        dev_release(p, &p->sp_Tg, (size_t)(p->sp_cap * p->sp_tg_map));
+        dev_release(p, &p->sp_V2f, (size_t)(p->sp_cap * p->sp_v2f_map));
+        dev_release(p, &p->sp_part, (size_t)(p->sp_cap * p->sp_pstride));
+        p->sp_cap = 0;
+        if ((st = dev_alloc(p, &p->sp_Tg, (size_t)(need * p->sp_tg_map))) ||
+            (st = dev_alloc(p, &p->sp_V2f, (size_t)(need * p->sp_v2f_map))) ||
+            (st = dev_alloc(p, &p->sp_part, (size_t)(need * p->sp_pstride))))
+            return st;
+        p->sp_cap = need;
     }
     if (!p->sp_dexp_valid) {
         for (int j = 0; j <= p->J; j++) {
@@ -773,7 +817,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
                        cudaStream_t s)
 {
     int st;
-    if ((st = split_prepare(p, s))) return st;
+    if ((st = split_prepare(p, nmaps, s))) return st;
     const int MAPS = split_maps_per_pass();
     const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
     const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
@@ -817,7 +861,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             a.dexp = p->sp_dexp + S.dexp_off;
             a.fexp = p->sp_fexp + S.fexp_off;
             a.fdig = p->sp_fdig + S.fdig_off;
-            a.Tg = p->sp_Tg + S.tg_off;
+            a.Tg = p->sp_Tg + p->sp_cap * S.tg_off;
             a.ph = p->sp_ph;
             a.tiles = S.tiles;
             a.ntiles = S.ntiles;
@@ -836,7 +880,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
                 ca.rows = p->N * bl;
                 ca.czt = p->czt[j][ca.mode];
                 ca.tw = p->tw.at(ca.czt.M);
-                ca.in_c = p->sp_Tg + S.tg_off + (long long)k * p->N * bl * bl;
+                ca.in_c = p->sp_Tg + p->sp_cap * S.tg_off + (long long)k * p->N * bl * bl;
                 ca.out_c = p->sp_Tb + S.tb_off;
                 {
                     KernelTimer kt(p, S2DWC_KIND_ANA_BETA, sj);
@@ -875,7 +919,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
                         cudaStream_t s)
 {
     int st;
-    if ((st = split_prepare(p, s))) return st;
+    if ((st = split_prepare(p, nmaps, s))) return st;
     const int MAPS = split_maps_per_pass();
     const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
     const long long bs2 = (long long)p->bl_scoeff * p->bl_scoeff;
@@ -908,7 +952,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
                 ca.tw = p->tw.at(ca.czt.M);
                 ca.in_c = p->sp_Tb + S.tb_off;
                 ca.in_r = nullptr;
-                ca.out_c = p->sp_V2f + S.v2f_off + k * S.vstride;
+                ca.out_c = p->sp_V2f + p->sp_cap * S.v2f_off + k * S.vstride;
                 ca.out_stride = p->gs_stride[j];
                 ca.wq = p->wq[j];
                 {
@@ -923,7 +967,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
             va.nch = S.snch;
             va.nmaps = nk;
             va.Vs = p->gs_stride[j];
-            va.V2f = p->sp_V2f + S.v2f_off;
+            va.V2f = p->sp_V2f + p->sp_cap * S.v2f_off;
             va.vstride = S.vstride;
             va.vexp = p->sp_vexp + S.fexp_off;
             va.vdig = p->sp_vdig + S.vdig_off;
@@ -1357,6 +1401,17 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
                                "stat_moments: scale %d has zero variance; its higher moments are set to zero", j);
     }
     return status;
+}
+
+int s2dwc_plan_reserve(s2dwc_plan *p, int nmaps, void *stream)
+{
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_reserve: null plan");
+    if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_reserve: nmaps=%d", nmaps);
+    if (p->form != S2DWC_FORM_SPLIT) return S2DWC_OK;
+    if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_reserve: tables not set");
+    DeviceGuard dg(p->device);
+    std::lock_guard<std::mutex> g(p->mu);
+    return split_prepare(p, nmaps, (cudaStream_t)stream);
 }
 
 int s2dwc_plan_check(s2dwc_plan *p)

@@ -157,6 +157,11 @@ class Plan:
                                             self._ptr(moments, torch.float64, n * (self.J + 1) * 6),
                                             self._stream(stream)))
 
+    def reserve(self, nmaps, stream=None):
+        """Sizes the split form's workspaces for batches of up to `nmaps`
+        maps (call before capturing batches in a CUDA graph)."""
+        check(lib().s2dwc_plan_reserve(self._h, int(nmaps), self._stream(stream)))
+
     def check(self):
         """Raises S2DWError if a split-form kernel gave up waiting (synchronises)."""
         check(lib().s2dwc_plan_check(self._h))

@@ -12,9 +12,17 @@ others are on the GPU overlaps on the device.  Each slot replays a CUDA graph
 captured once per (kind, input buffer), which removes the per-kernel launch
 cost of the ~20-70 kernels a transform issues.
 
+With ``form="split"`` the slots run the split-precision plan, whose
+tensor-core pass shares the Wigner-d digits among up to 32 maps: a free slot
+takes every waiting request of its configuration and kind (up to the slot's
+batch capacity) as one batch.  The batch's inputs are copied into the slot's
+staging buffers, so one CUDA graph per (kind, batch size) serves every batch.
+
 Results are identical alone and in a mix: the kernels are deterministic (no
-atomics; the synthesis sums scales in a fixed order), and a slot's buffers are
-owned by one request at a time.
+atomics; the synthesis sums scales in a fixed order), a slot's buffers are
+owned by one batch at a time, and in the split form each map's digits are
+scaled by that map's own exponents, so a map's result does not depend on the
+other maps of its batch.
 
 Latency of a request = device time of its completion event minus its arrival
 time, both relative to the stream's start (an event recorded when the first
@@ -47,37 +55,74 @@ class Request:
     out: object = None        # host copy of the output when keep_outputs
 
 
+def split_batch_capacity(B, N, alpha, J, max_batch=32, batch_bytes=2 << 30):
+    """Maps per batch of a split-form slot: up to `max_batch`, with the
+    slot's packed wavelet buffer within `batch_bytes`."""
+    return max(1, min(max_batch, int(batch_bytes) // (8 * _wav_size(B, N, alpha, J))))
+
+
 class Slot:
-    def __init__(self, key, tables, device):
+    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=2 << 30):
         import torch
 
         B, N, alpha, J = key
         self.key = key
-        self.plan = Plan(B, N, alpha, J, device=device)
+        self.split = form == "split"
+        self.cap = split_batch_capacity(B, N, alpha, J, max_batch, batch_bytes) if self.split else 1
+        self.plan = Plan(B, N, alpha, J, device=device, form=Plan.SPLIT if self.split else Plan.FP64)
         self.plan.set_tables(tables["K_gamma"], tables["Phi2"], tables["Slm"], tables["bl_scoeff"])
         bs = tables["bl_scoeff"]
         self.stream = torch.cuda.Stream(device=device)
-        self.d_wav = torch.empty(self.plan.wav_size, dtype=torch.float64, device=device)
-        self.d_sc = torch.empty(max(1, bs * bs), dtype=torch.complex128, device=device)
-        self.d_flm = torch.empty((B, B), dtype=torch.complex128, device=device)
-        self.bytes = self.plan.workspace_bytes() + 8 * self.plan.wav_size + 16 * (bs * bs + B * B)
+        c = self.cap
+        self.d_wav = torch.empty((c, self.plan.wav_size), dtype=torch.float64, device=device)
+        self.d_sc = torch.empty((c, max(1, bs * bs)), dtype=torch.complex128, device=device)
+        self.d_flm = torch.empty((c, B, B), dtype=torch.complex128, device=device)
+        staged = 0
+        if self.split:
+            # analysis inputs are staged here; synthesis inputs in d_wav / d_sc
+            self.in_flm = torch.empty((c, B, B), dtype=torch.complex128, device=device)
+            staged = 16 * c * B * B
+            self.plan.reserve(c, stream=self.stream)
+            self.stream.synchronize()
+        self.bytes = (self.plan.workspace_bytes() + 8 * c * self.plan.wav_size + 16 * c * (max(1, bs * bs) + B * B)
+                      + staged)
         self.graphs = {}
         self.busy = False
         self.last_used = 0.0
 
-    def run(self, req, use_graphs):
-        """Enqueue the request's transform on this slot's stream."""
+    def run(self, reqs, use_graphs):
+        """Enqueue the transform of a batch of requests (one request in the
+        FP64 form; same kind, at most `cap`) on this slot's stream."""
         import torch
 
+        kind, k = reqs[0].kind, len(reqs)
+        if self.split:
+            with torch.cuda.stream(self.stream):
+                for i, r in enumerate(reqs):
+                    if kind == "analysis":
+                        self.in_flm[i].copy_(r.inp[0], non_blocking=True)
+                    else:
+                        self.d_wav[i].copy_(r.inp[0], non_blocking=True)
+                        self.d_sc[i].copy_(r.inp[1].reshape(-1), non_blocking=True)
+
         def body():
-            if req.kind == "analysis":
-                self.plan.analysis(req.inp[0], self.d_wav, self.d_sc, stream=torch.cuda.current_stream())
+            cs = torch.cuda.current_stream()
+            if self.split:
+                if kind == "analysis":
+                    self.plan.analysis_batch(self.in_flm[:k], self.d_wav[:k], self.d_sc[:k], stream=cs)
+                else:
+                    self.plan.synthesis_batch(self.d_wav[:k], self.d_sc[:k], self.d_flm[:k], stream=cs)
+            elif kind == "analysis":
+                self.plan.analysis(reqs[0].inp[0], self.d_wav[0], self.d_sc[0], stream=cs)
             else:
-                self.plan.synthesis(req.inp[0], req.inp[1], self.d_flm, stream=torch.cuda.current_stream())
+                self.plan.synthesis(reqs[0].inp[0], reqs[0].inp[1], self.d_flm[0], stream=cs)
 
         with torch.cuda.stream(self.stream):
             if use_graphs:
-                gkey = (req.kind,) + tuple(t.data_ptr() for t in req.inp)
+                if self.split:
+                    gkey = (kind, k)
+                else:
+                    gkey = (kind,) + tuple(t.data_ptr() for t in reqs[0].inp)
                 g = self.graphs.get(gkey)
                 if g is None:
                     body()  # warm-up launch outside capture (lazy kernel attributes)
@@ -92,8 +137,9 @@ class Slot:
             ev.record(self.stream)
         return ev
 
-    def output(self, req):
-        return (self.d_wav, self.d_sc) if req.kind == "analysis" else (self.d_flm,)
+    def output(self, req, i=0):
+        """Output tensors of the i-th request of the batch that just ran."""
+        return (self.d_wav[i], self.d_sc[i]) if req.kind == "analysis" else (self.d_flm[i],)
 
     def close(self):
         self.graphs.clear()
@@ -102,7 +148,12 @@ class Slot:
 
 class Server:
     def __init__(self, hbm_budget_bytes=40 << 30, max_inflight=64, slots_per_config=2, use_graphs=True,
-                 device=0, keep_outputs=False):
+                 device=0, keep_outputs=False, form="fp64", max_batch=32, batch_bytes=2 << 30):
+        if form not in ("fp64", "split"):
+            raise ValueError(f"form must be 'fp64' or 'split', not {form!r}")
+        self.form = form
+        self.max_batch = max_batch
+        self.batch_bytes = batch_bytes
         self.budget = int(hbm_budget_bytes)
         self.max_inflight = max_inflight
         self.slots_per_config = slots_per_config
@@ -137,11 +188,11 @@ class Server:
             return None
         B, N, alpha, J = key
         # size estimate of a new slot; evict idle slots of other configs if needed
-        est = Slot.estimate_bytes(B, N, alpha, J)
+        est = Slot.estimate_bytes(B, N, alpha, J, self.form, self.max_batch, self.batch_bytes)
         while self.used + est > self.budget:
             if not self._evict_one(key):
                 return None
-        s = Slot(key, self.config_tables(B, N, alpha, J), self.device)
+        s = Slot(key, self.config_tables(B, N, alpha, J), self.device, self.form, self.max_batch, self.batch_bytes)
         self.slots[key].append(s)
         self.used += s.bytes
         return s
@@ -156,6 +207,7 @@ class Server:
         waiting = collections.deque()
         inflight = []
         done = []
+        batches = []
         base = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -177,22 +229,39 @@ class Server:
                 if s is None:
                     still.append(r)
                     continue
+                batch = [r]
+                if s.cap > 1:
+                    # the later waiting requests of the same configuration and kind
+                    rest_w = collections.deque()
+                    for r2 in waiting:
+                        if (len(batch) < s.cap and r2.kind == r.kind
+                                and (r2.B, r2.N, r2.alpha, r2.J) == key):
+                            batch.append(r2)
+                        else:
+                            rest_w.append(r2)
+                    waiting = rest_w
                 s.busy = True
                 s.last_used = now
-                r.slot_key = key
-                r.done_event = s.run(r, self.use_graphs)
-                inflight.append((r, s))
+                ev = s.run(batch, self.use_graphs)
+                for rb in batch:
+                    rb.slot_key = key
+                    rb.done_event = ev
+                inflight.append((batch, s))
+                batches.append(len(batch))
             waiting = still
             rest = []
-            for r, s in inflight:
-                if r.done_event.query():
-                    r.t_done = base.elapsed_time(r.done_event) / 1e3
-                    if self.keep_outputs:
-                        r.out = tuple(t.detach().cpu().numpy().copy() for t in s.output(r))
+            for batch, s in inflight:
+                ev = batch[0].done_event
+                if ev.query():
+                    t_done = base.elapsed_time(ev) / 1e3
+                    for i, rb in enumerate(batch):
+                        rb.t_done = t_done
+                        if self.keep_outputs:
+                            rb.out = tuple(t.detach().cpu().numpy().copy() for t in s.output(rb, i))
+                        done.append(rb)
                     s.busy = False
-                    done.append(r)
                 else:
-                    rest.append((r, s))
+                    rest.append((batch, s))
             inflight = rest
             if not inflight and not waiting and pending:
                 delay = pending[0].arrival - (time.perf_counter() - t0)
@@ -206,7 +275,8 @@ class Server:
         span = max(r.t_done for r in done) - min(r.arrival for r in done)
         return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
-                "throughput_rps": len(done) / span, "wall_s": t_end,
+                "throughput_rps": len(done) / span, "wall_s": t_end, "form": self.form,
+                "batches": len(batches), "mean_batch": float(np.mean(batches)) if batches else 0.0,
                 "slots": sum(len(v) for v in self.slots.values()), "hbm_bytes": self.used}
 
     def close(self):
@@ -217,20 +287,32 @@ class Server:
         self.used = 0
 
 
-def _estimate_bytes(B, N, alpha, J):
-    """Device bytes a slot of (B, N, alpha, J) holds (plan + buffers)."""
+def _wav_size(B, N, alpha, J):
     from .core import band_limits
 
-    wav = 0
-    tg = ta = 0
+    return sum((2 * bl - 1) * 2 * bl * N for bl, _ in (band_limits(j, B, alpha) for j in range(J + 1)))
+
+
+def _estimate_bytes(B, N, alpha, J, form="fp64", max_batch=32, batch_bytes=2 << 30):
+    """Device bytes a slot of (B, N, alpha, J) holds (plan + buffers); for
+    the split form with the map workspaces and staging of its batch."""
+    from .core import band_limits
+
+    wav = _wav_size(B, N, alpha, J)
+    tg = ta = sq = 0
     for j in range(J + 1):
         bl, _ = band_limits(j, B, alpha)
-        wav += (2 * bl - 1) * 2 * bl * N
         tg += N * bl * bl
         ta += N * bl * 2 * bl
+        sq += bl * bl
     Bp = (B + 31) // 32 * 32
     tables = B * Bp * 8 * 6 + B * B * 8 * 8 + B * B * 16
-    return 8 * wav + 16 * (tg + ta) * 3 // 2 + tables + 16 * B * B * 3
+    fp64 = 8 * wav + 16 * (tg + ta) * 3 // 2 + tables + 16 * B * B * 3
+    if form != "split":
+        return fp64
+    c = split_batch_capacity(B, N, alpha, J, max_batch, batch_bytes)
+    digits = 2 * 12 * 64 * sq + 2 * 2 * N * sq  # map digits of both directions, exponent tables
+    return fp64 + digits + c * (8 * wav + 16 * (tg + 2 * ta) + 16 * 2 * B * B)
 
 
 Slot.estimate_bytes = staticmethod(_estimate_bytes)

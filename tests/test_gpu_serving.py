@@ -58,3 +58,40 @@ def test_budget_evicts_idle_slots():
     assert stats["requests"] == len(reqs)
     assert srv.used <= small
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_split_form_batches_and_results_identical_alone(use_graphs):
+    """Split-form serving: waiting requests of one configuration and kind run
+    as one tensor-core batch; each result equals the result of the same
+    request served alone (a batch of one), bit for bit, and the FP64 form's
+    within the split form's tolerance (1e-10 relative to the largest output)."""
+    from s2dw_b200.serving import Server, make_stream
+
+    reqs, inputs = make_stream(48, seed=11, rate_hz=50000.0, Bs=(32, 64, 128), Ns=(2, 5), alphas=(2.0,), pool=2)
+    srv = Server(hbm_budget_bytes=16 << 30, slots_per_config=1, use_graphs=use_graphs, keep_outputs=True,
+                 form="split")
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats["requests"] == len(reqs)
+    assert stats["form"] == "split"
+    assert stats["mean_batch"] > 1.0
+    assert 0 < stats["p50_ms"] <= stats["p99_ms"]
+    mixed = {r.rid: r.out for r in reqs}
+
+    alone_srv = Server(hbm_budget_bytes=16 << 30, slots_per_config=1, use_graphs=False, keep_outputs=True,
+                       form="split")
+    fp64_srv = Server(hbm_budget_bytes=16 << 30, slots_per_config=1, use_graphs=False, keep_outputs=True)
+    for r in reqs:
+        r.arrival = 0.0
+        r.out = None
+        alone_srv.run([r])
+        for a, b in zip(r.out, mixed[r.rid]):
+            np.testing.assert_array_equal(a, b)
+        r.out = None
+        fp64_srv.run([r])
+        for a, b in zip(r.out, mixed[r.rid]):
+            assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max()
+    alone_srv.close()
+    fp64_srv.close()
