@@ -731,6 +731,22 @@ __device__ __forceinline__ int pos_of(int i, int R, int t, int lgM)
     return (r << lgM) + j + (s << lper);
 }
 
+// 32-byte accesses of the alpha stages (the two b columns of a b pair at
+// one (g, m)): one 256-bit access instead of two 128-bit ones halves the
+// L1 wavefronts of these row-strided loads and stores.  The streamed input
+// is not kept in L1, which holds the chirp tables.
+__device__ __forceinline__ void ld_pair(const double2 *p, double2 &a, double2 &b)
+{
+    asm("ld.global.nc.L1::no_allocate.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+        : "l"(p));
+}
+__device__ __forceinline__ void st_pair(double2 *p, double2 a, double2 b)
+{
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+                 : "memory");
+}
+
 // Input element k of transform `row` of a MODE transform (pre-chirp or
 // pre-twiddle applied); zero outside the transform's input range.
 template <int MODE>
@@ -743,7 +759,8 @@ __device__ __forceinline__ double2 fft_load(const CztArgs &a, int row, int k, co
         const int g = row / bl, bp = row % bl;
         const bool lo = k < bl;
         const double2 *p = a.in_c + ((size_t)g * bl + (lo ? k : n - k)) * (2 * bl) + 2 * bp;
-        double2 x1 = p[0], x2 = p[1];
+        double2 x1, x2;
+        ld_pair(p, x1, x2);
         const double2 pr = a.czt.pre[k];
         if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
         if (k == 0) { x1.y = 0.0; x2.y = 0.0; }
@@ -867,9 +884,8 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
             const double2 Zc = cconj(cmul(buf[padix((r << lgM) + mc)], a.czt.post[mc]));
             const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
             const double hh = 0.5 * a.scale;
-            double2 *p = a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * bp;
-            p[0] = make_double2(sm.x * hh, sm.y * hh);
-            p[1] = make_double2(d.y * hh, -d.x * hh);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * bp, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
         }
         return;
     }
@@ -1062,7 +1078,8 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
             if (k < n) {
                 const bool lo = k < bl;
                 const double2 *p = a.in_c + ((size_t)g * bl + (lo ? k : n - k)) * (2 * bl) + 2 * rr;
-                double2 x1 = p[0], x2 = p[1];
+                double2 x1, x2;
+                ld_pair(p, x1, x2);
                 if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
                 if (k == 0) { x1.y = 0.0; x2.y = 0.0; }
                 x = cmul(make_double2(x1.x - x2.y, x1.y + x2.x), a.czt.pre[k]);
@@ -1139,9 +1156,8 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
             const double2 Zc = cconj(cmul(buf[padix(mc)], a.czt.post[mc]));
             const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
             const double hh = 0.5 * a.scale;
-            double2 *p = a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr;
-            p[0] = make_double2(sm.x * hh, sm.y * hh);
-            p[1] = make_double2(d.y * hh, -d.x * hh);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
         }
         return;
     }
