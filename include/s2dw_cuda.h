@@ -277,6 +277,52 @@ int s2dwc_plan_set_timing(s2dwc_plan *plan, int enable);
 int s2dwc_plan_timing(s2dwc_plan *plan, int kind, long long *launches, double *total_ms);
 int s2dwc_plan_timing_reset(s2dwc_plan *plan);
 
+/* ---- Wavelet coefficient files (src/mod/s2dw_fileio_mod.f90) ----------
+ * Host-side writers and readers of the reference's FITS and Matlab wavelet
+ * files, so that coefficients computed here are read by the reference's
+ * programs and the other way round.  Arguments keep the reference's order;
+ * scoeff is complex128 (bl_scoeff x bl_scoeff), wav the static layout,
+ * wav_scales the dynamic one.  Writers fail with S2DWC_ERROR_FILEIO if the
+ * file exists, as the reference's do.  The reference's readers allocate
+ * their outputs; here the caller reads the sizes with the _read_header
+ * function first, allocates, and passes the same J, B, N, bl_scoeff to the
+ * data reader (S2DWC_ERROR_SIZE_INVALID if they differ from the file's).
+ * Readers report S2DWC_ERROR_FILEIO for a missing file, a wrong number of
+ * HDUs, inconsistent sizes or null coefficients, the reference's checks. */
+
+/* FITS: s2dw_fileio_fits_wav_write_dynamic, fileio:956-1079 */
+int s2dwc_fileio_fits_wav_write_dynamic(double *const *wav_scales, const double *scoeff, int J, int B, int N,
+                                        int bl_scoeff, double alpha, const char *filename, const char *comment);
+/* FITS: s2dw_fileio_fits_wav_write_static, fileio:796-926 */
+int s2dwc_fileio_fits_wav_write_static(const double *wav, const double *scoeff, int J, int B, int N, int bl_scoeff,
+                                       double alpha, const char *filename, const char *comment);
+/* The keywords s2dw_fileio_fits_wav_read_* start with (fileio:1325-1340). */
+int s2dwc_fileio_fits_wav_read_header(const char *filename, int *J, int *B, int *N, int *bl_scoeff,
+                                      double *alpha);
+/* FITS: s2dw_fileio_fits_wav_read_dynamic, fileio:1286-1435 */
+int s2dwc_fileio_fits_wav_read_dynamic(double *const *wav_scales, double *scoeff, int J, int B, int N,
+                                       int bl_scoeff, const char *filename);
+/* FITS: s2dw_fileio_fits_wav_read_static, fileio:1109-1253 */
+int s2dwc_fileio_fits_wav_read_static(double *wav, double *scoeff, int J, int B, int N, int bl_scoeff,
+                                      const char *filename);
+/* Matlab: s2dw_fileio_matlab_wav_write_dynamic, fileio:298-436 (writes
+ * filename, <base>_scoeff.dat and <base>_wcoeff.dat, base = filename
+ * without ".m") */
+int s2dwc_fileio_matlab_wav_write_dynamic(double *const *wav_scales, const double *scoeff, int J, int B, int N,
+                                          int bl_scoeff, double alpha, const char *filename, const char *comment);
+/* Matlab: s2dw_fileio_matlab_wav_write_static, fileio:102-268 */
+int s2dwc_fileio_matlab_wav_write_static(const double *wav, const double *scoeff, int J, int B, int N,
+                                         int bl_scoeff, double alpha, const char *filename, const char *comment);
+/* The parameters s2dw_fileio_matlab_wav_read_* start with (fileio:660-680). */
+int s2dwc_fileio_matlab_wav_read_header(const char *filename, int *J, int *B, int *N, int *bl_scoeff,
+                                        double *alpha);
+/* Matlab: s2dw_fileio_matlab_wav_read_dynamic, fileio:637-763 */
+int s2dwc_fileio_matlab_wav_read_dynamic(double *const *wav_scales, double *scoeff, int J, int B, int N,
+                                         int bl_scoeff, const char *filename);
+/* Matlab: s2dw_fileio_matlab_wav_read_static, fileio:473-601 */
+int s2dwc_fileio_matlab_wav_read_static(double *wav, double *scoeff, int J, int B, int N, int bl_scoeff,
+                                        const char *filename);
+
 #ifdef __cplusplus
 }
 #endif

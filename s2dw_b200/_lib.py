@@ -52,6 +52,18 @@ SIGNATURES = {
     "s2dwc_plan_set_timing": (_i, [_vp, _i]),
     "s2dwc_plan_timing": (_i, [_vp, _i, _llp, _dp]),
     "s2dwc_plan_timing_reset": (_i, [_vp]),
+    "s2dwc_fileio_fits_wav_write_dynamic": (_i, [ctypes.POINTER(_dp), _dp, _i, _i, _i, _i, _d, ctypes.c_char_p,
+                                                 ctypes.c_char_p]),
+    "s2dwc_fileio_fits_wav_write_static": (_i, [_dp, _dp, _i, _i, _i, _i, _d, ctypes.c_char_p, ctypes.c_char_p]),
+    "s2dwc_fileio_fits_wav_read_header": (_i, [ctypes.c_char_p, _ip, _ip, _ip, _ip, _dp]),
+    "s2dwc_fileio_fits_wav_read_dynamic": (_i, [ctypes.POINTER(_dp), _dp, _i, _i, _i, _i, ctypes.c_char_p]),
+    "s2dwc_fileio_fits_wav_read_static": (_i, [_dp, _dp, _i, _i, _i, _i, ctypes.c_char_p]),
+    "s2dwc_fileio_matlab_wav_write_dynamic": (_i, [ctypes.POINTER(_dp), _dp, _i, _i, _i, _i, _d, ctypes.c_char_p,
+                                                   ctypes.c_char_p]),
+    "s2dwc_fileio_matlab_wav_write_static": (_i, [_dp, _dp, _i, _i, _i, _i, _d, ctypes.c_char_p, ctypes.c_char_p]),
+    "s2dwc_fileio_matlab_wav_read_header": (_i, [ctypes.c_char_p, _ip, _ip, _ip, _ip, _dp]),
+    "s2dwc_fileio_matlab_wav_read_dynamic": (_i, [ctypes.POINTER(_dp), _dp, _i, _i, _i, _i, ctypes.c_char_p]),
+    "s2dwc_fileio_matlab_wav_read_static": (_i, [_dp, _dp, _i, _i, _i, _i, ctypes.c_char_p]),
 }
 
 KERNEL_KINDS = ["lwalk", "mwalk", "ana_beta", "ana_alpha", "syn_alpha", "syn_beta", "other"]

@@ -10,7 +10,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libs2dw_cuda.so")
-SOURCES = ["s2dw_host.cpp", "s2dw_kernels.cu", "s2dw_plan.cu", "s2dw_noalloc.cu", "s2dw_split.cu", "s2dw_stats.cu"]
+SOURCES = ["s2dw_host.cpp", "s2dw_kernels.cu", "s2dw_plan.cu", "s2dw_noalloc.cu", "s2dw_split.cu", "s2dw_stats.cu",
+           "s2dw_fileio.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
