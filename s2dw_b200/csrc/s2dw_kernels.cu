@@ -1180,6 +1180,91 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
 }
 
 // ===========================================================================
+// Synthesis alpha stage with the input prefetched (M = 4096, 8192)
+//
+// A persistent form of fft_large_kernel<CZT_SYN_ALPHA>: each CTA loops over
+// rows (g, b pair) and copies the next row's input (the two real rows of
+// the b pair: 2n contiguous doubles) into shared memory with cp.async while
+// the current row's two transforms run, so the input's DRAM latency is
+// hidden behind the FFT arithmetic instead of stalling every warp of the
+// CTA at the start of each row.  The twiddle tables are loaded once per CTA.
+// ===========================================================================
+__device__ __forceinline__ void pf_cp16(void *smem, const void *gmem)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void pf_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void pf_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Issues the copies of row r's input into stg: rows 2 rr and 2 rr + 1 of
+// scale g's wavelet block, 2n contiguous doubles starting at a multiple of
+// 2n doubles from in_r (16-byte aligned when in_r is).
+template <int THREADS>
+__device__ __forceinline__ void pf_prefetch(const CztArgs &a, int r, double2 *stg, int t)
+{
+    const int bl = a.bl, n = 2 * bl - 1, g = r / bl, rr = r - g * bl;
+    const double2 *base = reinterpret_cast<const double2 *>(a.in_r + (size_t)n * (2 * rr + (size_t)2 * bl * g));
+    for (int i = t; i < n; i += THREADS) pf_cp16(stg + i, base + i);
+}
+
+template <int LGM>
+__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_syn_alpha_pf_kernel(CztArgs a)
+{
+    constexpr int M = 1 << LGM, THREADS = M / 16;
+    extern __shared__ double2 smem[];
+    double2 *buf = smem;
+    double2 *twh = smem + padix(M) + 1;
+    double2 *twl = twh + M / 64;
+    double2 *stg = twl + 64;  // n double2 = the 2n doubles of the two real rows
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = 2 * bl - 1, rows = a.rows;
+    const double2 zero = make_double2(0.0, 0.0);
+
+    for (int i = t; i < M / 64; i += THREADS) twh[i] = a.tw.hi[i];
+    for (int i = t; i < 64; i += THREADS) twl[i] = a.tw.lo[i];
+    if ((int)blockIdx.x < rows) pf_prefetch<THREADS>(a, blockIdx.x, stg, t);
+    pf_commit();
+
+    for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+        const int g = r / bl, rr = r - g * bl;
+        pf_wait_all();
+        __syncthreads();  // row r staged; the previous row's reads of buf done
+        const double *sd = reinterpret_cast<const double *>(stg);
+        double2 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int k = lpos<LGM, 16>(t, i);
+            v[i] = (k < n) ? cmul(make_double2(sd[k], sd[n + k]), a.czt.pre[k]) : zero;
+        }
+        __syncthreads();  // staging free: copy the next row while this one runs
+        if (r + (int)gridDim.x < rows) pf_prefetch<THREADS>(a, r + gridDim.x, stg, t);
+        pf_commit();
+
+        fft_large<LGM, -1>(v, buf, t, twh, twl);
+        constexpr int RF = (LGM == 13) ? 2 : 16;
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], a.czt.Hf[lpos<LGM, RF>(t, i)]);
+        fft_large<LGM, +1>(v, buf, t, twh, twl);
+
+        // pair split through shared memory, as fft_large_kernel
+#pragma unroll
+        for (int i = 0; i < 16; i++) buf[padix(lpos<LGM, 16>(t, i))] = v[i];
+        __syncthreads();
+        for (int m = t; m < bl; m += THREADS) {
+            const int mc = (m == 0) ? 0 : n - m;
+            const double2 Z = cmul(buf[padix(m)], a.czt.post[m]);
+            const double2 Zc = cconj(cmul(buf[padix(mc)], a.czt.post[mc]));
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            const double hh = 0.5 * a.scale;
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+    pf_wait_all();
+}
+
+// ===========================================================================
 // Small kernels
 // ===========================================================================
 __global__ void zero_kernel(double *p, long long n)
@@ -1447,6 +1532,40 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
 }
 
 static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
+static bool g_alpha_prefetch = true;  // synthesis alpha stage: persistent kernel with prefetched input
+
+// Persistent synthesis alpha-stage launch: as many CTAs as fit on the
+// device at once, each looping over rows.
+template <int LGM>
+static int launch_syn_alpha_pf(const CztArgs &a, cudaStream_t s)
+{
+    constexpr int M = 1 << LGM, THREADS = M / 16;
+    const int n = 2 * a.bl - 1;
+    if (2 * n > 2 * M) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha stage: bl=%d does not fit M=%d", a.bl, M);
+    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + (size_t)n);
+    static int resident[64] = {0};
+    static size_t smem_set[64] = {0};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64) return set_error(S2DWC_ERROR_ARG_INVALID, "device index %d", dev);
+    if (smem_set[dev] < smem) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_syn_alpha_pf_kernel<LGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        int per_sm = 0, sms = 0;
+        S2DW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_syn_alpha_pf_kernel<LGM>, THREADS,
+                                                                    smem));
+        S2DW_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        resident[dev] = std::max(1, per_sm) * sms;
+        smem_set[dev] = smem;
+    }
+    const int grid = std::min(a.rows, resident[dev]);
+    if (grid <= 0) return S2DWC_OK;
+    fft_syn_alpha_pf_kernel<LGM><<<grid, THREADS, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+void set_alpha_prefetch(bool on) { g_alpha_prefetch = on; }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
@@ -1454,6 +1573,17 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
     if (M < 16 || M > 8192 || (M & (M - 1)))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "transform size %d unsupported", M);
     if (a.rows % a.bl == 0 && g_fft_values != 0) {
+        // Synthesis alpha stage: persistent kernel with the two real input
+        // rows (contiguous, copied in 16-byte chunks) prefetched; 4% faster
+        // than one row per CTA at bl = 1024.  The analysis alpha stage stays
+        // one row per CTA: its row-strided input gathered by cp.async gave
+        // no gain over 256-bit loads (the chirp-table loads from L2, not the
+        // input, dominate its remaining memory stalls).
+        const bool aligned = ((uintptr_t)a.in_r & 15) == 0;
+        if (g_alpha_prefetch && aligned && a.mode == CZT_SYN_ALPHA) {
+            if (M == 4096) return launch_syn_alpha_pf<12>(a, s);
+            if (M == 8192) return launch_syn_alpha_pf<13>(a, s);
+        }
         if (M == 4096) return launch_large<12>(a, s);
         if (M == 8192) return launch_large<13>(a, s);
     }

@@ -229,9 +229,15 @@ int plan_build(s2dwc_plan *p)
                 CztDev d;
                 d.M = c.M;
                 d.spec = c;
-                if ((st = dev_upload(p, &d.pre, pre)) || (st = dev_upload(p, &d.post, post)) ||
-                    (st = dev_upload(p, &d.Hf, Hf)))
+                if ((st = dev_upload(p, &d.pre, pre)) || (st = dev_upload(p, &d.Hf, Hf))) return st;
+                // the alpha stages' two chirps are the same table (K = Bout,
+                // no offsets): one copy, so that the kernels' table reads
+                // share their L1 lines
+                if (c.K == c.Bout && c.k0x2 == c.b0x2) {
+                    d.post = d.pre;
+                } else if ((st = dev_upload(p, &d.post, post))) {
                     return st;
+                }
                 arr[md] = d;
                 if (!p->tw.count(c.M)) {
                     std::vector<double2> hi, lo;
@@ -1079,6 +1085,10 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         return set_error(S2DWC_ERROR_ARG_INVALID, "device %d out of range (%d devices)", device, ndev);
     DeviceGuard dg(device);
     if (const char *fv = getenv("S2DW_FFT_VALUES")) set_fft_values(atoi(fv));
+    {
+        const char *ap = getenv("S2DW_ALPHA_PREFETCH");
+        set_alpha_prefetch(ap ? atoi(ap) != 0 : true);
+    }
     {
         const char *lw = getenv("S2DW_LWALK_VARIANT"), *mw = getenv("S2DW_MWALK_VARIANT");
         set_walk_variants(lw ? atoi(lw) : 0, mw ? atoi(mw) : 0);

@@ -93,3 +93,36 @@ def test_large_linearity():
     for x, y, z in zip(w1, w2, w3):
         scale = max(np.abs(x).max(), np.abs(y).max(), 1e-300)
         assert np.abs(z - (x - 2.0 * y)).max() <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha", [(1024, 4, 2.0), (2048, 2, 2.0)])
+def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
+    """The persistent synthesis alpha-stage kernel (input prefetched into
+    shared memory) does the same arithmetic as the one-row-per-CTA kernel:
+    the synthesis agrees bit for bit (M = 4096 and 8192)."""
+    from s2dw_b200.device import Plan
+
+    import torch
+
+    t = transform_setup(B, N, alpha)
+    flm = gaussian_flm(B, seed=2)
+    d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
+    out = {}
+    for pf in ("1", "0"):
+        monkeypatch.setenv("S2DW_ALPHA_PREFETCH", pf)
+        p = Plan(B, N, alpha, t["J"])
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+        w = torch.empty(p.wav_size, dtype=torch.float64, device="cuda")
+        sc = torch.empty(max(1, t["bl_scoeff"] ** 2), dtype=torch.complex128, device="cuda")
+        f = torch.empty_like(d_flm)
+        p.analysis(d_flm, w, sc)
+        p.synthesis(w, sc, f)
+        torch.cuda.synchronize()
+        out[pf] = (w.cpu().numpy(), f.cpu().numpy())
+        p.close()
+    monkeypatch.setenv("S2DW_ALPHA_PREFETCH", "1")
+    Plan(16, 2, 2.0, core.s2dw_core_comp_Jmax(16, 2.0)).close()  # restore the default for later tests
+    np.testing.assert_array_equal(out["1"][0], out["0"][0])
+    np.testing.assert_array_equal(out["1"][1], out["0"][1])
+    assert np.abs(out["1"][1].T - flm).max() <= 1e-10
