@@ -747,6 +747,17 @@ __device__ __forceinline__ void st_pair(double2 *p, double2 a, double2 b)
                  : "memory");
 }
 
+// Filter spectrum entry k of a Bluestein transform.  The alpha stages' filter
+// h(d) = conj(chirp(d)) is even in d (no offsets), so its spectrum is even:
+// Hf[k] = Hf[M - k]; reading only k <= M/2 halves the table's cache
+// footprint (32 KB instead of 64 KB at M = 4096).
+template <int MODE>
+__device__ __forceinline__ double2 hf_at(const double2 *Hf, int k, int M)
+{
+    if (MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA) return Hf[k <= (M >> 1) ? k : M - k];
+    return Hf[k];
+}
+
 // Input element k of transform `row` of a MODE transform (pre-chirp or
 // pre-twiddle applied); zero outside the transform's input range.
 template <int MODE>
@@ -845,7 +856,7 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
         fft_run<V, -1>(v, buf, t, lgM, Pf, twh, twl);
         const int RF = Pf.r(Pf.np - 1);
 #pragma unroll
-        for (int i = 0; i < V; i++) v[i] = cmul(v[i], a.czt.Hf[pos_of<V>(i, RF, t, lgM) & (M - 1)]);
+        for (int i = 0; i < V; i++) v[i] = cmul(v[i], hf_at<MODE>(a.czt.Hf, pos_of<V>(i, RF, t, lgM) & (M - 1), M));
         fft_run<V, +1>(v, buf, t, lgM, Pi, twh, twl);
         RL = Pi.r(Pi.np - 1);
     }
@@ -1125,7 +1136,7 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
         fft_large<LGM, -1>(v, buf, t, twh, twl);
         constexpr int RF = (LGM == 13) ? 2 : 16;
 #pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], a.czt.Hf[lpos<LGM, RF>(t, i)]);
+        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<MODE>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
         fft_large<LGM, +1>(v, buf, t, twh, twl);
     }
 
@@ -1244,7 +1255,7 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_syn_
         fft_large<LGM, -1>(v, buf, t, twh, twl);
         constexpr int RF = (LGM == 13) ? 2 : 16;
 #pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], a.czt.Hf[lpos<LGM, RF>(t, i)]);
+        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<CZT_SYN_ALPHA>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
         fft_large<LGM, +1>(v, buf, t, twh, twl);
 
         // pair split through shared memory, as fft_large_kernel
