@@ -180,7 +180,7 @@ int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
 void set_fft_values(int v);
-void set_alpha_prefetch(bool on);  // synthesis alpha stage: persistent kernel with prefetched input (default on)
+void set_alpha_prefetch(bool on);  // synthesis alpha / analysis beta stages: persistent kernel with prefetched input (default on)
 void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels  // FFT engine variant: 8 or 16 values per thread
 int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);

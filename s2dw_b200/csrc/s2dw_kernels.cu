@@ -1191,14 +1191,18 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
 }
 
 // ===========================================================================
-// Synthesis alpha stage with the input prefetched (M = 4096, 8192)
+// Stages with the input prefetched (M = 4096, 8192): synthesis alpha and
+// analysis beta
 //
-// A persistent form of fft_large_kernel<CZT_SYN_ALPHA>: each CTA loops over
-// rows (g, b pair) and copies the next row's input (the two real rows of
-// the b pair: 2n contiguous doubles) into shared memory with cp.async while
-// the current row's two transforms run, so the input's DRAM latency is
-// hidden behind the FFT arithmetic instead of stalling every warp of the
-// CTA at the start of each row.  The twiddle tables are loaded once per CTA.
+// A persistent form of fft_large_kernel for the two modes whose input row is
+// contiguous in HBM: each CTA loops over rows and copies the next row's input
+// into shared memory with cp.async while the current row's transforms run,
+// so the input's DRAM latency is hidden behind the FFT arithmetic instead of
+// stalling every warp of the CTA at the start of each row.  The twiddle
+// tables are loaded once per CTA.  Staged input per row:
+//   CZT_SYN_ALPHA (row = (g, b pair)): the two real rows of the b pair,
+//     2n contiguous doubles at a multiple of 2n doubles from in_r;
+//   FFT_ANA_BETA (row = (g, m)): Tg(g, m, 0..bl-1), bl complex values.
 // ===========================================================================
 __device__ __forceinline__ void pf_cp16(void *smem, const void *gmem)
 {
@@ -1208,68 +1212,106 @@ __device__ __forceinline__ void pf_cp16(void *smem, const void *gmem)
 __device__ __forceinline__ void pf_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void pf_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Issues the copies of row r's input into stg: rows 2 rr and 2 rr + 1 of
-// scale g's wavelet block, 2n contiguous doubles starting at a multiple of
-// 2n doubles from in_r (16-byte aligned when in_r is).
-template <int THREADS>
+// 16-byte chunks of one row's staged input.
+template <int MODE>
+__host__ __device__ constexpr int pf_chunks(int bl)
+{
+    return MODE == CZT_SYN_ALPHA ? 2 * bl - 1 : bl;
+}
+
+// Issues the copies of row r's input into stg.
+template <int MODE, int THREADS>
 __device__ __forceinline__ void pf_prefetch(const CztArgs &a, int r, double2 *stg, int t)
 {
     const int bl = a.bl, n = 2 * bl - 1, g = r / bl, rr = r - g * bl;
-    const double2 *base = reinterpret_cast<const double2 *>(a.in_r + (size_t)n * (2 * rr + (size_t)2 * bl * g));
-    for (int i = t; i < n; i += THREADS) pf_cp16(stg + i, base + i);
+    const double2 *base;
+    if (MODE == CZT_SYN_ALPHA)
+        base = reinterpret_cast<const double2 *>(a.in_r + (size_t)n * (2 * rr + (size_t)2 * bl * g));
+    else
+        base = a.in_c + ((size_t)g * bl + rr) * bl;
+    for (int i = t; i < pf_chunks<MODE>(bl); i += THREADS) pf_cp16(stg + i, base + i);
 }
 
-template <int LGM>
-__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_syn_alpha_pf_kernel(CztArgs a)
+template <int MODE, int LGM>
+__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_kernel(CztArgs a)
 {
+    static_assert(MODE == CZT_SYN_ALPHA || MODE == FFT_ANA_BETA, "contiguous-input stages only");
     constexpr int M = 1 << LGM, THREADS = M / 16;
+    // first-pass radix of the transform run first (as fft_large_kernel)
+    constexpr int R0 = (LGM == 13 && MODE == FFT_ANA_BETA) ? 2 : 16;
     extern __shared__ double2 smem[];
     double2 *buf = smem;
     double2 *twh = smem + padix(M) + 1;
     double2 *twl = twh + M / 64;
-    double2 *stg = twl + 64;  // n double2 = the 2n doubles of the two real rows
+    double2 *stg = twl + 64;
     const int t = threadIdx.x;
-    const int bl = a.bl, n = 2 * bl - 1, rows = a.rows;
+    const int bl = a.bl, n = 2 * bl - 1, rows = a.rows, N = a.N, Bout = a.czt.spec.Bout;
     const double2 zero = make_double2(0.0, 0.0);
 
     for (int i = t; i < M / 64; i += THREADS) twh[i] = a.tw.hi[i];
     for (int i = t; i < 64; i += THREADS) twl[i] = a.tw.lo[i];
-    if ((int)blockIdx.x < rows) pf_prefetch<THREADS>(a, blockIdx.x, stg, t);
+    if ((int)blockIdx.x < rows) pf_prefetch<MODE, THREADS>(a, blockIdx.x, stg, t);
     pf_commit();
 
     for (int r = blockIdx.x; r < rows; r += gridDim.x) {
         const int g = r / bl, rr = r - g * bl;
         pf_wait_all();
         __syncthreads();  // row r staged; the previous row's reads of buf done
-        const double *sd = reinterpret_cast<const double *>(stg);
         double2 v[16];
+        if (MODE == CZT_SYN_ALPHA) {
+            const double *sd = reinterpret_cast<const double *>(stg);
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int k = lpos<LGM, 16>(t, i);
-            v[i] = (k < n) ? cmul(make_double2(sd[k], sd[n + k]), a.czt.pre[k]) : zero;
+            for (int i = 0; i < 16; i++) {
+                const int k = lpos<LGM, R0>(t, i);
+                v[i] = (k < n) ? cmul(make_double2(sd[k], sd[n + k]), a.czt.pre[k]) : zero;
+            }
+        } else {  // k = m' mod 4bl, as fft_large_kernel's FFT_ANA_BETA load
+            const bool flip = (rr + N - 1) & 1;
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int k = lpos<LGM, R0>(t, i);
+                double2 x = zero;
+                if (k < bl) {
+                    x = cmul(stg[k], a.czt.pre[k]);
+                } else if (k > 3 * bl) {
+                    const int pp = 4 * bl - k;
+                    x = stg[pp];
+                    if (flip) x = make_double2(-x.x, -x.y);
+                    x = cmul(x, cconj(a.czt.pre[pp]));
+                }
+                v[i] = x;
+            }
         }
         __syncthreads();  // staging free: copy the next row while this one runs
-        if (r + (int)gridDim.x < rows) pf_prefetch<THREADS>(a, r + gridDim.x, stg, t);
+        if (r + (int)gridDim.x < rows) pf_prefetch<MODE, THREADS>(a, r + gridDim.x, stg, t);
         pf_commit();
 
-        fft_large<LGM, -1>(v, buf, t, twh, twl);
-        constexpr int RF = (LGM == 13) ? 2 : 16;
+        if (MODE == CZT_SYN_ALPHA) {
+            fft_large<LGM, -1>(v, buf, t, twh, twl);
+            constexpr int RF = (LGM == 13) ? 2 : 16;
 #pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<CZT_SYN_ALPHA>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
-        fft_large<LGM, +1>(v, buf, t, twh, twl);
-
-        // pair split through shared memory, as fft_large_kernel
+            for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<MODE>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
+            fft_large<LGM, +1>(v, buf, t, twh, twl);
+            // pair split through shared memory, as fft_large_kernel
 #pragma unroll
-        for (int i = 0; i < 16; i++) buf[padix(lpos<LGM, 16>(t, i))] = v[i];
-        __syncthreads();
-        for (int m = t; m < bl; m += THREADS) {
-            const int mc = (m == 0) ? 0 : n - m;
-            const double2 Z = cmul(buf[padix(m)], a.czt.post[m]);
-            const double2 Zc = cconj(cmul(buf[padix(mc)], a.czt.post[mc]));
-            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
-            const double hh = 0.5 * a.scale;
-            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
-                    make_double2(d.y * hh, -d.x * hh));
+            for (int i = 0; i < 16; i++) buf[padix(lpos<LGM, 16>(t, i))] = v[i];
+            __syncthreads();
+            for (int m = t; m < bl; m += THREADS) {
+                const int mc = (m == 0) ? 0 : n - m;
+                const double2 Z = cmul(buf[padix(m)], a.czt.post[m]);
+                const double2 Zc = cconj(cmul(buf[padix(mc)], a.czt.post[mc]));
+                const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+                const double hh = 0.5 * a.scale;
+                st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                        make_double2(d.y * hh, -d.x * hh));
+            }
+        } else {
+            fft_large<LGM, +1>(v, buf, t, twh, twl);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int b = lpos<LGM, 16>(t, i);
+                if (b < Bout) a.out_c[((size_t)g * bl + rr) * (2 * bl) + b] = v[i];
+            }
         }
     }
     pf_wait_all();
@@ -1543,35 +1585,34 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
 }
 
 static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
-static bool g_alpha_prefetch = true;  // synthesis alpha stage: persistent kernel with prefetched input
+static bool g_alpha_prefetch = true;  // contiguous-input stages: persistent kernel with prefetched input
 
-// Persistent synthesis alpha-stage launch: as many CTAs as fit on the
+// Persistent launch of the prefetching stages: as many CTAs as fit on the
 // device at once, each looping over rows.
-template <int LGM>
-static int launch_syn_alpha_pf(const CztArgs &a, cudaStream_t s)
+template <int MODE, int LGM>
+static int launch_pf(const CztArgs &a, cudaStream_t s)
 {
     constexpr int M = 1 << LGM, THREADS = M / 16;
-    const int n = 2 * a.bl - 1;
-    if (2 * n > 2 * M) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha stage: bl=%d does not fit M=%d", a.bl, M);
-    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + (size_t)n);
+    const int chunks = pf_chunks<MODE>(a.bl);
+    if (chunks > M) return set_error(S2DWC_ERROR_SIZE_INVALID, "prefetch stage: bl=%d does not fit M=%d", a.bl, M);
+    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + (size_t)chunks);
     static int resident[64] = {0};
     static size_t smem_set[64] = {0};
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64) return set_error(S2DWC_ERROR_ARG_INVALID, "device index %d", dev);
     if (smem_set[dev] < smem) {
-        S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_syn_alpha_pf_kernel<LGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_pf_kernel<MODE, LGM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
         int per_sm = 0, sms = 0;
-        S2DW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_syn_alpha_pf_kernel<LGM>, THREADS,
-                                                                    smem));
+        S2DW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pf_kernel<MODE, LGM>, THREADS, smem));
         S2DW_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         resident[dev] = std::max(1, per_sm) * sms;
         smem_set[dev] = smem;
     }
     const int grid = std::min(a.rows, resident[dev]);
     if (grid <= 0) return S2DWC_OK;
-    fft_syn_alpha_pf_kernel<LGM><<<grid, THREADS, smem, s>>>(a);
+    fft_pf_kernel<MODE, LGM><<<grid, THREADS, smem, s>>>(a);
     S2DW_CUDA_TRY(cudaGetLastError());
     return S2DWC_OK;
 }
@@ -1584,16 +1625,19 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
     if (M < 16 || M > 8192 || (M & (M - 1)))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "transform size %d unsupported", M);
     if (a.rows % a.bl == 0 && g_fft_values != 0) {
-        // Synthesis alpha stage: persistent kernel with the two real input
-        // rows (contiguous, copied in 16-byte chunks) prefetched; 4% faster
-        // than one row per CTA at bl = 1024.  The analysis alpha stage stays
-        // one row per CTA: its row-strided input gathered by cp.async gave
-        // no gain over 256-bit loads (the chirp-table loads from L2, not the
-        // input, dominate its remaining memory stalls).
-        const bool aligned = ((uintptr_t)a.in_r & 15) == 0;
-        if (g_alpha_prefetch && aligned && a.mode == CZT_SYN_ALPHA) {
-            if (M == 4096) return launch_syn_alpha_pf<12>(a, s);
-            if (M == 8192) return launch_syn_alpha_pf<13>(a, s);
+        // Stages whose input row is contiguous: persistent kernel with the
+        // next row prefetched (synthesis alpha 4% faster than one row per
+        // CTA at bl = 1024).  The analysis alpha stage stays one row per
+        // CTA: its row-strided input gathered by cp.async gave no gain over
+        // 256-bit loads (the chirp-table loads from L2, not the input,
+        // dominate its remaining memory stalls).
+        if (g_alpha_prefetch && a.mode == CZT_SYN_ALPHA && ((uintptr_t)a.in_r & 15) == 0) {
+            if (M == 4096) return launch_pf<CZT_SYN_ALPHA, 12>(a, s);
+            if (M == 8192) return launch_pf<CZT_SYN_ALPHA, 13>(a, s);
+        }
+        if (g_alpha_prefetch && a.mode == FFT_ANA_BETA && ((uintptr_t)a.in_c & 15) == 0) {
+            if (M == 4096) return launch_pf<FFT_ANA_BETA, 12>(a, s);
+            if (M == 8192) return launch_pf<FFT_ANA_BETA, 13>(a, s);
         }
         if (M == 4096) return launch_large<12>(a, s);
         if (M == 8192) return launch_large<13>(a, s);

@@ -98,9 +98,10 @@ def test_large_linearity():
 @pytest.mark.gpu
 @pytest.mark.parametrize("B,N,alpha", [(1024, 4, 2.0), (2048, 2, 2.0)])
 def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
-    """The persistent synthesis alpha-stage kernel (input prefetched into
-    shared memory) does the same arithmetic as the one-row-per-CTA kernel:
-    the synthesis agrees bit for bit (M = 4096 and 8192)."""
+    """The persistent kernels of the synthesis alpha and analysis beta stages
+    (next row's input prefetched into shared memory) do the same arithmetic
+    as the one-row-per-CTA kernel: wavelets and synthesis agree bit for bit
+    (M = 4096 and 8192)."""
     from s2dw_b200.device import Plan
 
     import torch
