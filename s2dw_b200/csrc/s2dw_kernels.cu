@@ -1442,7 +1442,16 @@ int launch_lwalk(const LwalkArgs &a, cudaStream_t s)
 {
     switch (g_lwalk_variant) {
     case 1: return launch_lwalk_s<4, 4>(a, s);
-    default: return launch_lwalk_s<4, 0>(a, s);
+    case 2: return launch_lwalk_s<4, 3>(a, s);
+    default:
+        // more resident CTAs where the register cap costs no spills and the
+        // grid is many waves deep (bl >= 1024: 2048+ tiles); measured on
+        // B200: NP = 2, bl = 1024: 3 CTAs/SM 10 % faster than 2; NP = 1:
+        // 4 CTAs/SM 4 % faster.  Smaller grids lose more to the tail wave,
+        // and NP >= 3 spills under the caps.
+        if (a.bl >= 1024 && a.NP == 2) return launch_lwalk_np<2, 4, 3>(a, s);
+        if (a.bl >= 1024 && a.NP == 1) return launch_lwalk_np<1, 4, 4>(a, s);
+        return launch_lwalk_s<4, 0>(a, s);
     }
 }
 
@@ -1489,7 +1498,11 @@ int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
 {
     switch (g_mwalk_variant) {
     case 1: return launch_mwalk_q<8, 0>(a, s);
-    default: return launch_mwalk_q<4, 4>(a, s);
+    case 2: return launch_mwalk_q<4, 5>(a, s);
+    case 3: return launch_mwalk_q<4, 4>(a, s);
+    // 3 CTAs/SM (<= 168 registers, no spills): 3-10 % faster than 4 CTAs/SM
+    // with 128 registers and small spills, at N = 1, 3, 4, 6, 8 (B200)
+    default: return launch_mwalk_q<4, 3>(a, s);
     }
 }
 
