@@ -33,12 +33,12 @@ METRIC = "B=1024 N=4 analysis+synthesis pairs/s at recon err<=1e-10"
 UNIT = "pairs/s"
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
-# kernel kind, averaged over the 66 launches of each kind in two
-# analysis+synthesis pairs at B=1024 N=4 alpha=2 J=10, from one ncu capture of
-# this script (command and per-kernel table: profiles/traffic_B1024_N4.md).
-# Used only for the roofline "traffic" entry of that workload.
-NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.43e6, "mwalk": 10.77e6, "ana_beta": 27.73e6,
-                                "ana_alpha": 45.15e6, "syn_alpha": 43.53e6, "syn_beta": 56.48e6}}
+# kernel kind, averaged over the 22 launches of each kind in two
+# analysis+synthesis pairs at B=1024 N=4 alpha=2 J=10 (11 scales), from one
+# ncu capture of this script.  Used only for the roofline "traffic" entry of
+# that workload.
+NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.60e6, "mwalk": 10.76e6, "ana_beta": 27.64e6,
+                                "ana_alpha": 45.15e6, "syn_alpha": 43.95e6, "syn_beta": 31.50e6}}
 
 
 def parse():
