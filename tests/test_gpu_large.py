@@ -56,7 +56,8 @@ def test_B256_N5_full_parity():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("B,N,alpha,power", [(1024, 4, 2.0, 1.0), (1024, 8, 3.0, 1.0), (2048, 8, 2.0, 1.2)])
+@pytest.mark.parametrize("B,N,alpha,power", [(1024, 4, 2.0, 1.0), (1024, 8, 3.0, 1.0), (2048, 8, 2.0, 1.2),
+                                             (700, 3, 2.5, 1.0)])
 def test_large_roundtrip_and_small_scale_parity(B, N, alpha, power):
     t = transform_setup(B, N, alpha)
     J = t["J"]
@@ -96,7 +97,7 @@ def test_large_linearity():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("B,N,alpha", [(1024, 4, 2.0), (2048, 2, 2.0)])
+@pytest.mark.parametrize("B,N,alpha", [(1024, 4, 2.0), (2048, 2, 2.0), (700, 3, 2.5), (1500, 2, 2.0)])
 def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
     """The persistent kernels of the synthesis alpha and analysis beta stages
     (next row's input prefetched into shared memory) do the same arithmetic
