@@ -6,8 +6,9 @@
 //   v(l; m', m, n)  = d^l_{m'm}(pi/2) d^l_{m'n}(pi/2) K_j(l) s(l, n),
 //
 // is, for a batch of maps k sharing (B, N, alpha, J), a GEMM over l whose
-// left operand v does not depend on the map: rows (m', n, +-) for one m,
-// columns (k, re/im).  Each CTA owns one m, CH consecutive m' ("chains") and
+// left operand v does not depend on the map: rows (m', n, l parity) for one
+// m, columns (k, re/im); the even-l and odd-l sums E, O give T(+n) = E + O
+// and T(-n) = E - O in the epilogue.  Each CTA owns one m, CH consecutive m' ("chains") and
 // up to 32 maps.  Per chunk of 32 values of l:
 //
 //   * one or two walker warps advance the FP64 l-recurrence of d^l_{m'm}
@@ -58,7 +59,7 @@ constexpr int E_ZERO = -32000;      // exponent of an all-zero row or column
 constexpr int E_MIN = -960;         // rows or columns below 2^E_MIN count as zero
 constexpr int THREADS = 128;
 
-// Chains per CTA: 2*NP rows per chain (n and +-), 128 rows, chains a multiple
+// Chains per CTA: 2*NP rows per chain (n and l parity), 128 rows, chains a multiple
 // of 16 so that every staged table row starts on a 128-byte boundary.
 __host__ __device__ constexpr int chains(int NP) { return NP == 1 ? 64 : (NP == 2 ? 32 : 16); }
 
@@ -168,15 +169,24 @@ __device__ __forceinline__ long long to_fixed(double x, double factor)
     return X;
 }
 
-// Byte d (0..DIG-1) of four fixed-point integers, packed into one word.
-__device__ __forceinline__ uint32_t pack4(const long long *X, int d)
+// The DIG digit words of four fixed-point integers: o[d] holds byte d of
+// X[0..3] in bytes 0..3.  A 4 x 4 byte transpose of the low words gives
+// digits 0-3 and a 4 x 2 one of the high words digits 4-5 (12 byte permutes).
+__device__ __forceinline__ void digits4(const long long *X, uint32_t (&o)[DIG])
 {
-    const int sh = d < 4 ? 0 : 32;
-    const uint32_t s0 = (uint32_t)(X[0] >> sh), s1 = (uint32_t)(X[1] >> sh), s2 = (uint32_t)(X[2] >> sh),
-                   s3 = (uint32_t)(X[3] >> sh);
-    const int b = d & 3;
-    const uint32_t sel = (uint32_t)(b | ((b + 4) << 4));
-    return __byte_perm(__byte_perm(s0, s1, sel), __byte_perm(s2, s3, sel), 0x5410);
+    static_assert(DIG == 6, "six byte digits");
+    const uint32_t w0 = (uint32_t)X[0], w1 = (uint32_t)X[1], w2 = (uint32_t)X[2], w3 = (uint32_t)X[3];
+    const uint32_t a = __byte_perm(w0, w1, 0x5140), b = __byte_perm(w2, w3, 0x5140);  // bytes 0, 1
+    const uint32_t c = __byte_perm(w0, w1, 0x7362), e = __byte_perm(w2, w3, 0x7362);  // bytes 2, 3
+    o[0] = __byte_perm(a, b, 0x5410);
+    o[1] = __byte_perm(a, b, 0x7632);
+    o[2] = __byte_perm(c, e, 0x5410);
+    o[3] = __byte_perm(c, e, 0x7632);
+    const uint32_t h0 = (uint32_t)(X[0] >> 32), h1 = (uint32_t)(X[1] >> 32), h2 = (uint32_t)(X[2] >> 32),
+                   h3 = (uint32_t)(X[3] >> 32);
+    const uint32_t f = __byte_perm(h0, h1, 0x5140), g = __byte_perm(h2, h3, 0x5140);  // bytes 4, 5
+    o[4] = __byte_perm(f, g, 0x5410);
+    o[5] = __byte_perm(f, g, 0x7632);
 }
 
 // 16 consecutive K values of one operand row -> the 16-byte K-half of each of
@@ -184,14 +194,31 @@ __device__ __forceinline__ uint32_t pack4(const long long *X, int d)
 // consecutive digit tiles are `tile` bytes apart.
 __device__ __forceinline__ void store_digits(unsigned char *base, int tile, const long long *X)
 {
+    uint32_t o0[DIG], o1[DIG], o2[DIG], o3[DIG];
+    digits4(X + 0, o0);
+    digits4(X + 4, o1);
+    digits4(X + 8, o2);
+    digits4(X + 12, o3);
+#pragma unroll
+    for (int d = 0; d < DIG; d++) *reinterpret_cast<uint4 *>(base + d * tile) = make_uint4(o0[d], o1[d], o2[d], o3[d]);
+}
+
+// As store_digits, split by the parity of the K index: row `even` gets the
+// values at even K positions (odd ones zero), row `odd` the others.  Byte j
+// of each digit word is K position 4w + j, so the parity masks are per byte.
+__device__ __forceinline__ void store_digits_parity(unsigned char *even, unsigned char *odd, int tile,
+                                                    const long long *X)
+{
+    uint32_t o0[DIG], o1[DIG], o2[DIG], o3[DIG];
+    digits4(X + 0, o0);
+    digits4(X + 4, o1);
+    digits4(X + 8, o2);
+    digits4(X + 12, o3);
+    constexpr uint32_t ME = 0x00FF00FFu, MO = 0xFF00FF00u;
 #pragma unroll
     for (int d = 0; d < DIG; d++) {
-        uint4 v;
-        v.x = pack4(X + 0, d);
-        v.y = pack4(X + 4, d);
-        v.z = pack4(X + 8, d);
-        v.w = pack4(X + 12, d);
-        *reinterpret_cast<uint4 *>(base + d * tile) = v;
+        *reinterpret_cast<uint4 *>(even + d * tile) = make_uint4(o0[d] & ME, o1[d] & ME, o2[d] & ME, o3[d] & ME);
+        *reinterpret_cast<uint4 *>(odd + d * tile) = make_uint4(o0[d] & MO, o1[d] & MO, o2[d] & MO, o3[d] & MO);
     }
 }
 
@@ -434,8 +461,9 @@ struct SplitSmem {
     static constexpr int WL = CH < 32 ? CH : 32;             // chains per walker warp
     static constexpr int NCUT_W = ISSUER_WARP - NWALK;        // cutter warps
     static constexpr int GEN = 0;                             // 2 stages x DIG x A_TILE
-    static constexpr int MAP = GEN + 2 * DIG * A_TILE;        // 2 stages x DIG x B_TILE
-    static constexpr int VB = MAP + 2 * DIG * B_TILE;         // 2 x [64 chains][33]
+    static constexpr int MAP_ST = 3;                          // map digit stages
+    static constexpr int MAP = GEN + 2 * DIG * A_TILE;        // MAP_ST stages x DIG x B_TILE
+    static constexpr int VB = MAP + MAP_ST * DIG * B_TILE;    // 2 x [64 chains][33]
     static constexpr int VB_ONE = 64 * 33;                    // doubles per buffer
     // walker tables, per walker warp and buffer (doubles): Ap[KC][WL], Am[KC], Om[KC]
     static constexpr int WT = VB + 2 * VB_ONE * 8;
@@ -445,8 +473,8 @@ struct SplitSmem {
     static constexpr int GT_DBL = KC * NP * CH;
     static constexpr int PH = GT + 2 * GT_DBL * 8;            // phases [g*16 + n+N-1]
     static constexpr int EF = PH + 8 * 16 * 16;               // column factors 2^(Ef - SHIFT)
-    static constexpr int BAR = EF + COLS * 8;                 // VFULL[2], CUT[2], full[2], done[2]
-    static constexpr int TM = BAR + 8 * 8;
+    static constexpr int BAR = EF + COLS * 8;                 // VFULL[2], CUT[2], full[3], done[2]
+    static constexpr int TM = BAR + 9 * 8;
     static constexpr int ABORT = TM + 8;
     static constexpr int BYTES = ABORT + 8 + 1024;            // + alignment slack
     static constexpr int TS_LD = COLS + 1;                    // epilogue tile row stride
@@ -478,7 +506,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
     auto vfull = [&](int b) { return bar0 + 8 * b; };
     auto cutb = [&](int b) { return bar0 + 16 + 8 * b; };
     auto full = [&](int b) { return bar0 + 32 + 8 * b; };
-    auto done = [&](int b) { return bar0 + 48 + 8 * b; };
+    auto done = [&](int b) { return bar0 + 56 + 8 * b; };
     // bounded wait that returns at once after an abort
     auto wait = [&](uint32_t bar, uint32_t parity) -> bool {
         if (*sAbort) return false;
@@ -509,9 +537,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         for (int i = 0; i < 2; i++) {
             mbar_init(vfull(i), NWALK);
             mbar_init(cutb(i), S::NCUT_W);
-            mbar_init(full(i), 1);
             mbar_init(done(i), 1);
         }
+        for (int i = 0; i < S::MAP_ST; i++) mbar_init(full(i), 1);
         mbar_fence_init();
         *sAbort = 0;
     }
@@ -645,10 +673,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
                     if (prow && l > blo) v = vb[pch * 33 + li] * T[(li * NP + pq) * CH + pch];
                     X[i] = to_fixed(v, dfac);
                 }
-                store_digits(gen + tile_off(ROWS, 2 * pair, kh), A_TILE, X);
-#pragma unroll
-                for (int i = 1; i < 16; i += 2) X[i] = -X[i];  // (-1)^l, l = 32c + 16kh + i
-                store_digits(gen + tile_off(ROWS, 2 * pair + 1, kh), A_TILE, X);
+                // rows 2 pair (even l) and 2 pair + 1 (odd l): the epilogue
+                // forms E + O and E - O, the +n and -n sums; l = 32c + 16kh + i
+                store_digits_parity(gen + tile_off(ROWS, 2 * pair, kh), gen + tile_off(ROWS, 2 * pair + 1, kh),
+                                    A_TILE, X);
                 fence_async_smem();
             }
             __syncwarp();
@@ -659,7 +687,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
     } else if (lane == 0 && nout > 0) {
         // ================= issuer =================
         auto map_copy = [&](int c) {
-            const int st = (c - c_start) & 1;
+            const int st = (c - c_start) % S::MAP_ST;
             mbar_expect_tx(full(st), DIG * B_TILE);
             bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
                      a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
@@ -669,16 +697,19 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         bool first_lev[LEV];
 #pragma unroll
         for (int i = 0; i < LEV; i++) first_lev[i] = true;
+        // Map digits run two chunks ahead in three stages: the copy for chunk
+        // k + 2 goes into the stage the MMAs of chunk k - 1 read, once those
+        // have finished, so that the MMAs of chunk k are issued without
+        // waiting for chunk k - 1's to complete.
         map_copy(c_start);
+        if (nout > 1) map_copy(c_start + 1);
         for (int k = 0; k < nout; k++) {
-            const int gs = k & 1, c = c_start + k;
+            const int gs = k & 1, ms = k % S::MAP_ST, c = c_start + k;
             if (!wait(cutb(gs), (k >> 1) & 1)) continue;
-            if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
-            if (k + 1 < nout) map_copy(c + 1);
-            if (!wait(full(gs), (k >> 1) & 1)) continue;
+            if (!wait(full(ms), (k / S::MAP_ST) & 1)) continue;
             tc_fence_after();
             const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
-            const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
+            const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + ms * DIG * B_TILE), COLS * 16, 128);
 #pragma unroll
             for (int i = 0; i < DIG; i++)
 #pragma unroll
@@ -692,6 +723,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
                     first_lev[lev] = false;
                 }
             mma_commit(done(gs));
+            if (k + 2 < nout) {
+                if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
+                map_copy(c + 2);
+            }
         }
         wait(done((nout - 1) & 1), ((nout - 1) >> 1) & 1);
     }
@@ -740,9 +775,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
 #pragma unroll
         for (int q = 0; q < NP; q++) {
             const int n = a.nq[q], pr = c * NP + q;
-            const double2 sum = make_double2(Ts[(2 * pr) * S::TS_LD + 2 * k], Ts[(2 * pr) * S::TS_LD + 2 * k + 1]);
-            const double2 dif =
+            // rows 2 pr and 2 pr + 1 hold the even-l and odd-l sums E, O
+            const double2 E = make_double2(Ts[(2 * pr) * S::TS_LD + 2 * k], Ts[(2 * pr) * S::TS_LD + 2 * k + 1]);
+            const double2 O =
                 make_double2(Ts[(2 * pr + 1) * S::TS_LD + 2 * k], Ts[(2 * pr + 1) * S::TS_LD + 2 * k + 1]);
+            const double2 sum = make_double2(E.x + O.x, E.y + O.y), dif = make_double2(E.x - O.x, E.y - O.y);
             if (n == 0) {
                 Tp[q] = c_ipow(sum, -m);
                 Tm[q] = make_double2(0.0, 0.0);
@@ -778,7 +815,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
 //
 // a GEMM per m with rows l (chains of the m'-recurrence, 128 per CTA), K over
 // (m', q) and columns (map, re/im).  Same digits, levels and TMEM layout as
-// the analysis; the walker warps cut their own rows (no +-n rows here).
+// the analysis; the walker warps cut their own rows (no parity rows here).
 // ===========================================================================
 __host__ __device__ constexpr int syn_npq(int NP) { return NP == 1 ? 1 : (NP == 2 ? 2 : 4); }
 __host__ __device__ constexpr int syn_mc(int NP) { return KC / syn_npq(NP); }
