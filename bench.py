@@ -290,7 +290,7 @@ def split_stats(B, N, alpha, J, maps, repeats=3, power=1.0):
             "kernels": contraction,
             "max_w_err": werr, "max_w_err_per_scale": per_scale, "max_flm_err_synthesis": synerr,
             "recon_err": recon, "recon_err_rel_max_flm": recon_rel,
-            "form": "split analysis and synthesis contractions (tcgen05 int8 digits, 6 bytes, 28 exact products); FP64 recurrences, tables and FFTs",
+            "form": "split analysis and synthesis contractions (tcgen05 int8 digits, 6 bytes, 26 exact products); FP64 recurrences, tables and FFTs",
             "workload": f"B={B} N={N} alpha={alpha:g} J={J}, {maps} seeded maps per batch"
                         + (f", C_l=(1/(l(l+1)))^{power:g}" if power != 1.0 else "") + ", device-resident"}
 

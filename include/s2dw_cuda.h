@@ -56,7 +56,7 @@ extern "C" {
 /* Precision form of the transform.  FP64: every stage in FP64, the drop-in
  * form.  SPLIT: the analysis and synthesis contractions run on the tensor
  * cores as exact int8 products of 48-bit fixed-point digits (six byte digits
- * per operand, per-row and per-column power-of-two scales, the 28 most
+ * per operand, per-row and per-column power-of-two scales, the 26 most
  * significant digit products summed exactly in int32), combined in FP64; the
  * d^l(pi/2) recurrences, the kernel tables and the beta/alpha transforms stay
  * FP64.  Its error is bounded by 1e-10 of max|w| per scale (analysis) and of

@@ -20,7 +20,7 @@
 //     no-swizzle operand layout;
 //   * the map operand (f^k(l, m), cut the same way by fdig_kernel, one scale
 //     per (m, k, re/im) column) arrives by a bulk copy;
-//   * one thread issues 28 tcgen05.mma.kind::i8 (M=128, N=64, K=32): the
+//   * one thread issues 26 tcgen05.mma.kind::i8 (M=128, N=64, K=32): the
 //     digit products of significance level t = (5-i)+(5-j) <= 6, each level
 //     into its own int32 TMEM accumulator, so every product is summed exactly.
 //
