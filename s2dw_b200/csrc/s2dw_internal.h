@@ -179,9 +179,9 @@ int launch_gprep(const GprepArgs &a, cudaStream_t s);
 int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp, cudaStream_t s);
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
-void set_fft_values(int v);
+void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread, 0 = general engine only
 void set_alpha_prefetch(bool on);  // synthesis alpha / analysis beta stages: persistent kernel with prefetched input (default on)
-void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels  // FFT engine variant: 8 or 16 values per thread
+void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels
 int launch_zero(double *p, long long n, cudaStream_t s);
 int launch_scoeff_copy(double2 *scoeff, const double2 *flm, int B, int bs, cudaStream_t s);
 int launch_scaling_add(double2 *flm, const double2 *scoeff, const double *Phi2, int B, int bs,

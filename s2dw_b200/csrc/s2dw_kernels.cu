@@ -1390,7 +1390,7 @@ static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 
 static int g_lwalk_variant = 0, g_mwalk_variant = 0;
 
-int lwalk_tile_m(int) { return LW_W * (g_lwalk_variant == 1 ? 4 : 4); }
+int lwalk_tile_m(int) { return LW_W * 4; }  // S = 4 pairs per thread in every variant
 int mwalk_tile_m(int) { return MW_W * (g_mwalk_variant == 1 ? 8 : 4); }
 
 void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t)
