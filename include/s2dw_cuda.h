@@ -159,7 +159,10 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
 int s2dwc_plan_destroy(s2dwc_plan *plan);
 
 /* Uploads the caller's kernel tables (host pointers, reference layouts).
- * Phi2 may be NULL for analysis-only use. */
+ * Phi2 may be NULL for analysis-only use.  Any complex Slm is accepted; one
+ * not of the form s2dw_core_init_directionality produces (S/eta real, eta = 1
+ * for odd N, i for even N) makes every FP64 contraction run twice, and the
+ * split form refuses it (S2DWC_ERROR_ARG_INVALID). */
 int s2dwc_plan_set_tables(s2dwc_plan *plan, const double *K_gamma, const double *Phi2,
                           const double *Slm, int bl_scoeff);
 

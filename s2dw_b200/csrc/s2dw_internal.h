@@ -115,6 +115,10 @@ struct LwalkArgs {
     double2 *Tg;          // [g][m][m'] N x bl x bl
     const int2 *tiles;    // (p-tile, m-tile) per CTA, longest walks first
     int ntiles;
+    // 0: Tg = T.  1: G holds the second real part b of S = eta (a + i b)
+    // (a general complex Slm): Tg += T with the +n terms times -i and the
+    // -n terms times +i (conj(S) for n >= 0, S for n < 0).
+    int acc_imag;
 };
 
 struct MwalkArgs {
@@ -130,6 +134,9 @@ struct MwalkArgs {
     double2 *part;        // this scale's flm contribution [(l-blo-1)*bl + m], m <= l
     const int2 *tiles;    // (l-tile, m-tile) per CTA, longest walks first
     int ntiles;
+    // 0: part = result.  1: G holds the second real part b of S = eta (a + i b)
+    // (a general complex Slm): part += i * result.
+    int acc_imag;
 };
 // Tile lists of the contraction kernels for one scale, ordered by decreasing
 // work so that the longest walks start first.

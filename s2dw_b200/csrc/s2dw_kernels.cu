@@ -278,12 +278,15 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
             const int n = a.nq[q];
             const double2 E = cscale(acc[0][s][q], sc), O = cscale(acc[1][s][q], sc);
             const double2 sum = cadd(E, O), dif = csub(E, O);
+            // acc_imag: the b part of S enters the +n terms times -i (i^-1)
+            // and the -n terms times +i
+            const int ai = a.acc_imag ? 1 : 0;
             if (n == 0) {
-                Tp[q] = cipow(sum, -m);
+                Tp[q] = cipow(sum, -m - ai);
                 Tm[q] = make_double2(0.0, 0.0);
             } else {
-                Tp[q] = cipow(sum, n - m - ev);
-                double2 t = cipow(dif, -n - m + ev);
+                Tp[q] = cipow(sum, n - m - ev - ai);
+                double2 t = cipow(dif, -n - m + ev + ai);
                 if ((mp + n) & 1) t = make_double2(-t.x, -t.y);
                 Tm[q] = t;
             }
@@ -296,7 +299,8 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
                 y = cadd(y, cmul(Tp[q], sPh[gg * 16 + n + N - 1]));
                 if (n != 0) y = cadd(y, cmul(Tm[q], sPh[gg * 16 - n + N - 1]));
             }
-            a.Tg[((size_t)gg * bl + m) * bl + mp] = y;
+            double2 *dst = a.Tg + ((size_t)gg * bl + m) * bl + mp;
+            *dst = a.acc_imag ? cadd(*dst, y) : y;
         }
     }
 }
@@ -523,7 +527,9 @@ __device__ __forceinline__ void mwalk_body(const MwalkArgs &a)
     for (int q = 0; q < Q; q++) {
         if (!val[q]) continue;
         const int m = mbase + w * Q + q;
-        a.part[(size_t)(l - blo - 1) * bl + m] = cipow(cscale(acc[q], sc), m);
+        double2 *dst = a.part + (size_t)(l - blo - 1) * bl + m;
+        if (a.acc_imag) *dst = cadd(*dst, cipow(cscale(acc[q], sc), m + 1));  // + i * result
+        else *dst = cipow(cscale(acc[q], sc), m);
     }
 }
 

@@ -44,6 +44,11 @@ struct s2dwc_plan {
     // caller tables folded into per-scale factor tables
     double *kappaA = nullptr, *kappaS = nullptr, *Phi2 = nullptr;
     double *Ga = nullptr, *Gsyn = nullptr;       // all scales, see LwalkArgs/MwalkArgs
+    // a general complex Slm, S = eta (a + i b) with b != 0: the tables of b
+    // (built on first use); the contractions then run twice (acc_imag)
+    bool slm_general = false;
+    long long ga_total = 0, gs_total = 0;
+    double *kappaA_b = nullptr, *kappaS_b = nullptr, *Ga_b = nullptr, *Gsyn_b = nullptr;
     std::vector<long long> ga_off, gs_off;       // per-scale offsets (doubles)
     std::vector<int> ga_stride, gs_stride;
     double2 *Fw = nullptr;                       // per-call F table [l*Bp + m]
@@ -299,6 +304,8 @@ int plan_build(s2dwc_plan *p)
         na += (long long)nl * p->NP * p->ga_stride[j];
         ns += (long long)nl * p->NP * p->gs_stride[j];
     }
+    p->ga_total = na;
+    p->gs_total = ns;
     if ((st = dev_alloc(p, &p->Ga, (size_t)std::max(1LL, na))) ||
         (st = dev_alloc(p, &p->Gsyn, (size_t)std::max(1LL, ns))) ||
         (st = dev_alloc(p, &p->Fw, (size_t)B * Bp)))
@@ -457,6 +464,12 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
             KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
             if ((st = launch_lwalk(la, sj))) return st;
         }
+        if (p->slm_general) {  // the b part of a general Slm, accumulated into Tg
+            la.G = p->Ga_b + p->ga_off[j];
+            la.acc_imag = 1;
+            KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
+            if ((st = launch_lwalk(la, sj))) return st;
+        }
         CztArgs ca{};
         ca.mode = p->ana_beta_mode[j];
         ca.bl = bl;
@@ -557,6 +570,12 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
             KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
             if ((st = launch_mwalk(ma, sj))) return st;
         }
+        if (p->slm_general) {  // the b part of a general Slm, accumulated into part
+            ma.G = p->Gsyn_b + p->gs_off[j];
+            ma.acc_imag = 1;
+            KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
+            if ((st = launch_mwalk(ma, sj))) return st;
+        }
         if (!p->timing) S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], sj));
     }
     if (!p->timing)
@@ -629,6 +648,11 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
         la.tiles = p->lw_tiles[j];
         la.ntiles = p->lw_ntiles[j];
         if ((st = launch_lwalk(la, s))) return st;
+        if (p->slm_general) {  // the b part of a general Slm, accumulated into Tg
+            la.G = p->Ga_b + p->ga_off[j];
+            la.acc_imag = 1;
+            if ((st = launch_lwalk(la, s))) return st;
+        }
         CztArgs ca{};
         ca.mode = p->ana_beta_mode[j];
         ca.bl = bl;
@@ -659,6 +683,9 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
 int split_prepare(s2dwc_plan *p, int nmaps, cudaStream_t s)
 {
     int st;
+    if (p->slm_general)
+        return set_error(S2DWC_ERROR_ARG_INVALID,
+                         "the split form needs Slm of the form s2dw_core_init_directionality produces (S/eta real)");
     const int NP = p->NP, CH = split_chains(NP), MAPS = split_maps_per_pass(), MC = split_syn_mc(NP);
     if (!p->sp_alloc) {
         p->sp.resize(p->J + 1);
@@ -1123,38 +1150,58 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
     if (bl_scoeff < 0 || bl_scoeff > B)
         return set_error(S2DWC_ERROR_SIZE_INVALID, "bl_scoeff=%d outside [0,B]", bl_scoeff);
     const std::complex<double> *S = reinterpret_cast<const std::complex<double> *>(Slm_);
-    // The kernels factor S(l,n) = s(l,n) * eta with eta = 1 (N odd) or i
-    // (N even), the form s2dw_core_init_directionality produces
-    // (s2dw_core_mod.f90:240-245).  Entries with N+n even are never used.
+    // The kernels factor S(l,n) = eta (a(l,n) + i b(l,n)) with eta = 1 (N odd)
+    // or i (N even) and a, b real.  s2dw_core_init_directionality produces
+    // b = 0 (s2dw_core_mod.f90:240-245); any other Slm (b != 0 somewhere)
+    // runs the contractions a second time with the tables of b.  Entries
+    // with N+n even are never used.
     const bool even = (N % 2 == 0);
-    std::vector<double> s((size_t)B * NP);
+    std::vector<double> sa((size_t)B * NP), sb((size_t)B * NP);
+    bool general = false;
     for (int q = 0; q < NP; q++)
         for (int l = 0; l < B; l++) {
-            std::complex<double> v = S[l + (size_t)B * p->nq[q]];
-            double other = even ? v.real() : v.imag();
-            if (other != 0.0)
-                return set_error(S2DWC_ERROR_ARG_INVALID,
-                                 "Slm(%d,%d) is not of the form s*%s produced by init_directionality",
-                                 l, p->nq[q], even ? "i" : "1");
-            s[(size_t)l * NP + q] = even ? v.imag() : v.real();
+            const std::complex<double> v = S[l + (size_t)B * p->nq[q]];
+            // S / eta: eta = i divides as (x + i y) / i = y - i x
+            sa[(size_t)l * NP + q] = even ? v.imag() : v.real();
+            sb[(size_t)l * NP + q] = even ? -v.real() : v.imag();
+            if (sb[(size_t)l * NP + q] != 0.0) general = true;
         }
-    std::vector<double> kA((size_t)(J + 1) * B * NP), kS((size_t)(J + 1) * B * NP);
-    const double c8 = 8.0 * (M_PI * M_PI);
-    for (int j = 0; j <= J; j++)
-        for (int l = 0; l < B; l++) {
-            const double K = K_gamma[j + (size_t)(J + 1) * l];
-            for (int q = 0; q < NP; q++) {
-                const int n = p->nq[q];
-                const double sv = s[(size_t)l * NP + q];
-                kA[((size_t)j * B + l) * NP + q] = K * sv;
-                // (2l+1)/(8 pi^2) (1 or 2) K S i^{-n} with the eta i^{-n}
-                // phase reduced to the real sign (-1)^floor(n/2)
-                const double sig = ((n / 2) & 1) ? -1.0 : 1.0;
-                kS[((size_t)j * B + l) * NP + q] =
-                    ((double)(2 * l + 1) / c8) * (n == 0 ? 1.0 : 2.0) * K * sv * sig;
+    auto factors = [&](const std::vector<double> &s, std::vector<double> &kA, std::vector<double> &kS) {
+        kA.assign((size_t)(J + 1) * B * NP, 0.0);
+        kS.assign((size_t)(J + 1) * B * NP, 0.0);
+        const double c8 = 8.0 * (M_PI * M_PI);
+        for (int j = 0; j <= J; j++)
+            for (int l = 0; l < B; l++) {
+                const double K = K_gamma[j + (size_t)(J + 1) * l];
+                for (int q = 0; q < NP; q++) {
+                    const int n = p->nq[q];
+                    const double sv = s[(size_t)l * NP + q];
+                    kA[((size_t)j * B + l) * NP + q] = K * sv;
+                    // (2l+1)/(8 pi^2) (1 or 2) K S i^{-n} with the eta i^{-n}
+                    // phase reduced to the real sign (-1)^floor(n/2)
+                    const double sig = ((n / 2) & 1) ? -1.0 : 1.0;
+                    kS[((size_t)j * B + l) * NP + q] =
+                        ((double)(2 * l + 1) / c8) * (n == 0 ? 1.0 : 2.0) * K * sv * sig;
+                }
             }
-        }
+    };
+    std::vector<double> kA, kS;
+    factors(sa, kA, kS);
     DeviceGuard dg(p->device);
+    if (general && !p->Ga_b) {
+        int st;
+        if ((st = dev_alloc(p, &p->kappaA_b, (size_t)(J + 1) * B * NP)) ||
+            (st = dev_alloc(p, &p->kappaS_b, (size_t)(J + 1) * B * NP)) ||
+            (st = dev_alloc(p, &p->Ga_b, (size_t)std::max(1LL, p->ga_total))) ||
+            (st = dev_alloc(p, &p->Gsyn_b, (size_t)std::max(1LL, p->gs_total))))
+            return st;
+    }
+    if (general) {
+        std::vector<double> kAb, kSb;
+        factors(sb, kAb, kSb);
+        S2DW_CUDA_TRY(cudaMemcpy(p->kappaA_b, kAb.data(), kAb.size() * sizeof(double), cudaMemcpyHostToDevice));
+        S2DW_CUDA_TRY(cudaMemcpy(p->kappaS_b, kSb.data(), kSb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     S2DW_CUDA_TRY(cudaMemcpy(p->kappaA, kA.data(), kA.size() * sizeof(double), cudaMemcpyHostToDevice));
     S2DW_CUDA_TRY(cudaMemcpy(p->kappaS, kS.data(), kS.size() * sizeof(double), cudaMemcpyHostToDevice));
     if (Phi2)
@@ -1181,9 +1228,22 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
         g.stride = p->gs_stride[j];
         g.out = p->Gsyn + p->gs_off[j];
         if ((st = launch_gprep(g, 0))) return st;
+        if (general) {
+            g.T = p->Om;
+            g.kappa = p->kappaA_b + (size_t)j * B * NP;
+            g.stride = p->ga_stride[j];
+            g.out = p->Ga_b + p->ga_off[j];
+            if ((st = launch_gprep(g, 0))) return st;
+            g.T = p->Gam;
+            g.kappa = p->kappaS_b + (size_t)j * B * NP;
+            g.stride = p->gs_stride[j];
+            g.out = p->Gsyn_b + p->gs_off[j];
+            if ((st = launch_gprep(g, 0))) return st;
+        }
     }
     S2DW_CUDA_TRY(cudaDeviceSynchronize());
     p->bl_scoeff = bl_scoeff;
+    p->slm_general = general;
     p->tables_set = true;
     p->sp_dexp_valid = false;
     return S2DWC_OK;
@@ -1201,9 +1261,11 @@ long long s2dwc_plan_workspace_bytes(const s2dwc_plan *p) { return p ? p->ws_byt
 int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
 {
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "launch_count: null plan");
-    if (analysis) *analysis = 3 * (p->J + 1) + 2;
+    // a general Slm runs each contraction twice
+    const int g = p->slm_general ? 2 : 1;
+    if (analysis) *analysis = (2 + g) * (p->J + 1) + 2;
     int ns = 1;
-    for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? 1 : 0);
+    for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? g : 0);
     if (synthesis) *synthesis = ns;
     return S2DWC_OK;
 }

@@ -193,3 +193,73 @@ def test_host_api_pinned_buffers_match_pageable():
                                                    bs, alpha)
     np.testing.assert_array_equal(out, ref)
     assert np.abs(out - flm).max() < 1e-12
+
+
+def _general_slm(B, N, seed):
+    """A complex Slm not of the init_directionality form: S(l,n) = eta (a + i b)
+    with both real parts nonzero (random, seeded), on the n the transform uses."""
+    rng = np.random.default_rng(seed)
+    S = np.zeros((B, N), dtype=np.complex128, order="F")
+    for n in range(N):
+        if (N + n) % 2 == 1:
+            S[n:, n] = rng.standard_normal(B - n) + 1j * rng.standard_normal(B - n)
+    return np.asfortranarray(S)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha", [(32, 3, 2.0), (40, 4, 2.5), (24, 1, 2.0), (32, 8, 3.0)])
+def test_general_complex_slm_matches_oracle(B, N, alpha):
+    """Any complex Slm (the reference's API accepts one): analysis and
+    synthesis against the oracle, whose loops take S as given
+    (s2dw_core_mod.f90:417-428, :1228-1253)."""
+    t = transform_setup(B, N, alpha)
+    S = _general_slm(B, N, seed=B + N)
+    flm = gaussian_flm(B, seed=7)
+    a = (t["K_gamma"], S, t["J"], B, N, t["bl_scoeff"], alpha)
+    s = (t["K_gamma"], t["Phi2"], S, t["J"], B, N, t["bl_scoeff"], alpha)
+    wav, sc = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+    wav_ref, sc_ref = O.analysis_dynamic(flm, *a)
+    for j, (w, r) in enumerate(zip(wav, wav_ref)):
+        if np.abs(r).max() > 0:
+            assert _rel(w, r) <= TOL, f"scale {j}: rel err {_rel(w, r):.3e}"
+    f = core.s2dw_core_synthesis_wav2flm_dynamic(list(wav_ref), sc_ref, *s)
+    f_ref = O.synthesis_dynamic(wav_ref, sc_ref, *s)
+    assert _rel(f, f_ref) <= TOL, f"synthesis rel err {_rel(f, f_ref):.3e}"
+
+
+@pytest.mark.gpu
+def test_general_slm_device_plan_and_split_rejection():
+    """The device plan with a general Slm agrees with the host entry point;
+    the no-allocation analysis runs the second contraction too; the split
+    form refuses such an Slm (S2DW_ERROR_ARG_INVALID)."""
+    import torch
+
+    from s2dw_b200._lib import S2DWError
+    from s2dw_b200.device import Plan
+
+    B, N, alpha = 32, 4, 2.0
+    t = transform_setup(B, N, alpha)
+    S = _general_slm(B, N, seed=3)
+    flm = gaussian_flm(B, seed=8)
+    wav_h, sc_h = core.s2dw_core_analysis_flm2wav_dynamic(flm, t["K_gamma"], S, t["J"], B, N, t["bl_scoeff"], alpha)
+    p = Plan(B, N, alpha, t["J"])
+    p.set_tables(t["K_gamma"], t["Phi2"], S, t["bl_scoeff"])
+    d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
+    w = torch.empty(p.wav_size, dtype=torch.float64, device="cuda")
+    w2 = torch.empty_like(w)
+    sc = torch.empty(max(1, t["bl_scoeff"] ** 2), dtype=torch.complex128, device="cuda")
+    p.analysis(d_flm, w, sc)
+    p.analysis_noalloc(d_flm, w2, sc)
+    torch.cuda.synchronize()
+    wn, wn2 = w.cpu().numpy(), w2.cpu().numpy()
+    offs = p.wav_offsets
+    for j in range(t["J"] + 1):
+        np.testing.assert_array_equal(wn[offs[j]:offs[j + 1]], wav_h[j].ravel(order="F"))
+    np.testing.assert_array_equal(wn2, wn)
+    p.close()
+    sp = Plan(B, N, alpha, t["J"], form=Plan.SPLIT)
+    sp.set_tables(t["K_gamma"], t["Phi2"], S, t["bl_scoeff"])
+    with pytest.raises(S2DWError) as e:
+        sp.analysis_batch(d_flm.reshape(1, B, B), w.reshape(1, -1), sc.reshape(1, -1))
+    assert e.value.code == 10
+    sp.close()
