@@ -293,9 +293,10 @@ static void split_mant_exp(ld v, double *mant, int32_t *ex)
     *ex = e - 1;
 }
 
-void build_rec_tables(int B, RecTables &t)
+void build_rec_tables(int B, int hn, RecTables &t)
 {
     t.B = B;
+    t.HN = hn;
     const size_t BB = (size_t)B * B;
     t.Om.assign(BB, 0.0);
     t.Acoef.assign(BB, 0.0);
@@ -305,7 +306,7 @@ void build_rec_tables(int B, RecTables &t)
     t.Bcoef.assign(BB, 0.0);
     t.Em.assign(BB, 0.0);
     t.Ee.assign(BB, 0);
-    t.H.assign(BB * 8, 0.0);
+    t.H.assign(BB * hn, 0.0);
 
     // Edge values E(l,k) = sqrt(C(2l,l+k))/2^l = |d^l_{l,k}(pi/2)| by exact
     // products (E(l,0)^2 = prod (2i-1)/(2i); E(l,k)/E(l,k-1) = sqrt((l-k+1)/(l+k))).
@@ -372,16 +373,16 @@ void build_rec_tables(int B, RecTables &t)
         }
     }
 
-    // H(l,m',n) = d^l_{m'n}(pi/2), n < 8, by the l recurrence in long double.
+    // H(l,m',n) = d^l_{m'n}(pi/2), n < hn, by the l recurrence in long double.
 #pragma omp parallel for schedule(dynamic, 8)
     for (int mp = 0; mp < B; mp++) {
-        for (int n = 0; n < 8 && n < B; n++) {
+        for (int n = 0; n < hn && n < B; n++) {
             int l0 = mp > n ? mp : n;
             ld d = (mp >= n) ? (((l0 - n) & 1) ? -E[(size_t)l0 * B + n] : E[(size_t)l0 * B + n])
                              : E[(size_t)l0 * B + mp];
             ld dp = 0.0L;
             for (int l = l0; l < B; l++) {
-                t.H[((size_t)l * 8 + n) * B + mp] = (double)d;
+                t.H[((size_t)l * hn + n) * B + mp] = (double)d;
                 ld dn;
                 if (l == 0) dn = 0.0L;
                 else dn = -u_of(l, mp) * u_of(l, n) * d - v_of(l, mp) * v_of(l, n) * dp;

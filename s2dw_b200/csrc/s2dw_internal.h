@@ -46,17 +46,22 @@ int positive_nset(int N, int *nq);
 // Start values are stored as mantissa (double in [1,2)) and binary exponent.
 // All 2-D tables are [l*B + x] with zeros where x > l.
 // ---------------------------------------------------------------------------
+// Azimuthal band limits: N <= S2DW_NMAX (FP64 form; the split form N <= 8),
+// so at most S2DW_NPMAX values n >= 0 with N + n odd.
+constexpr int S2DW_NMAX = 16;
+constexpr int S2DW_NPMAX = S2DW_NMAX / 2;
+
 struct RecTables {
-    int B = 0;
+    int B = 0, HN = 8;
     std::vector<double> Om, Acoef;     // l-walk scale chains and coefficients
     std::vector<double> Stm;           // l-walk start E(l0,k)/Om_l0(k) mantissa
     std::vector<int32_t> Ste;          //   ... exponent
     std::vector<double> Gam, Bcoef;    // m'-walk chains and coefficients
     std::vector<double> Em;            // edge values E(l,m)=sqrt(C(2l,l+m))/2^l
     std::vector<int32_t> Ee;
-    std::vector<double> H;             // d^l_{m'n}(pi/2), n<8: [(l*8+n)*B + m']
+    std::vector<double> H;             // d^l_{m'n}(pi/2), n < HN: [(l*HN+n)*B + m']
 };
-void build_rec_tables(int B, RecTables &t);
+void build_rec_tables(int B, int hn, RecTables &t);  // H for n < hn
 
 // ---------------------------------------------------------------------------
 // Chirp-z (Bluestein) transform specification:
@@ -105,7 +110,7 @@ struct TwDev {
 // 32-wide tiles never read past a row.
 struct LwalkArgs {
     int B, Bp, N, NP, bl, blo;
-    int nq[4];
+    int nq[S2DW_NPMAX];
     const double *Acoef;  // [l*Bp + x]
     const double *Stm;    // [l0*B + k]
     const int32_t *Ste;
@@ -123,7 +128,7 @@ struct LwalkArgs {
 
 struct MwalkArgs {
     int B, Bp, N, NP, bl, blo;
-    int nq[4];
+    int nq[S2DW_NPMAX];
     const double *Bcoef;  // [l*Bp + m']
     const double *Em;     // [l*B + m]
     const int32_t *Ee;
@@ -161,14 +166,14 @@ struct CombineArgs {
 // set_tables time: out[((l-blo-1)*NP+q)*stride + x] = T[l*Bp+x] *
 // H[(l*8+nq)*B+x] * kappa[l*NP+q] for x <= l, x < bl; zero elsewhere.
 struct GprepArgs {
-    int B, Bp, NP, bl, blo, stride;
-    int nq[4];
+    int B, Bp, NP, bl, blo, stride, hn;  // hn: n rows of H
+    int nq[S2DW_NPMAX];
     const double *T, *H, *kappa;
     double *out;
 };
 struct CztArgs {
     int mode, bl, N, NP, rows;
-    int nq[4];
+    int nq[S2DW_NPMAX];
     CztDev czt;
     TwDev tw;
     const double2 *in_c;   // complex input (Tg, Tb, V)
@@ -206,7 +211,7 @@ int launch_combine(const CombineArgs &a, cudaStream_t s);
 struct SplitArgs {
     int B, Bp, N, NP, bl, blo;
     int c0, nch, nmaps;        // first 32-row chunk of l stored in fdig, chunks, maps (<= 32)
-    int nq[4];
+    int nq[S2DW_NPMAX];
     const double *Acoef, *Om;  // [l*Bp + x]
     const double *Stm;         // [l0*B + k]
     const int32_t *Ste;

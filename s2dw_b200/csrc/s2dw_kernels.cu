@@ -84,6 +84,7 @@ __device__ __forceinline__ void cp_wait()
 // ===========================================================================
 constexpr int LW_W = 4;    // warps per CTA
 constexpr int LW_CH = 16;  // l values per staged chunk (even)
+constexpr int LW_PHS = 2 * S2DW_NMAX;  // gamma-DFT phase table row: n + N - 1 < 2N - 1
 
 template <int NP, int S>
 struct LwalkSmem {
@@ -94,7 +95,7 @@ struct LwalkSmem {
     static constexpr int G_OFF = AP_OFF + LW_CH * 32;
     static constexpr int AM_OFF = G_OFF + LW_CH * NP * 32;
     static constexpr int BUF = AM_OFF + LW_CH * WS;
-    static constexpr size_t BYTES = 2 * BUF * sizeof(double) + 8 * 16 * sizeof(double2);
+    static constexpr size_t BYTES = 2 * BUF * sizeof(double) + S2DW_NMAX * LW_PHS * sizeof(double2);
 };
 
 template <int NP, int S>
@@ -103,7 +104,7 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
     using L = LwalkSmem<NP, S>;
     constexpr int WS = L::WS;
     extern __shared__ __align__(16) double lsm[];
-    double2 *sPh = reinterpret_cast<double2 *>(lsm + 2 * L::BUF);  // [g*16 + n+N-1]
+    double2 *sPh = reinterpret_cast<double2 *>(lsm + 2 * L::BUF);  // [g*LW_PHS + n+N-1]
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int2 tile = a.tiles[blockIdx.x];
@@ -115,7 +116,7 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
         const int g = i / (2 * N - 1), n = i % (2 * N - 1) - (N - 1);
         double sn, cs;
         sincospi((double)(n * g) / (double)N, &sn, &cs);
-        sPh[g * 16 + n + N - 1] = make_double2(cs, sn);
+        sPh[g * LW_PHS + n + N - 1] = make_double2(cs, sn);
     }
 
     // ---- per-pair start values; pair = (m' = mp, m = m0 + w*S + s)
@@ -296,8 +297,8 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
 #pragma unroll
             for (int q = 0; q < NP; q++) {
                 const int n = a.nq[q];
-                y = cadd(y, cmul(Tp[q], sPh[gg * 16 + n + N - 1]));
-                if (n != 0) y = cadd(y, cmul(Tm[q], sPh[gg * 16 - n + N - 1]));
+                y = cadd(y, cmul(Tp[q], sPh[gg * LW_PHS + n + N - 1]));
+                if (n != 0) y = cadd(y, cmul(Tm[q], sPh[gg * LW_PHS - n + N - 1]));
             }
             double2 *dst = a.Tg + ((size_t)gg * bl + m) * bl + mp;
             *dst = a.acc_imag ? cadd(*dst, y) : y;
@@ -330,7 +331,7 @@ __global__ void gprep_kernel(GprepArgs a)
         const int q = (int)(r % a.NP), l = a.blo + 1 + (int)(r / a.NP);
         double v = 0.0;
         if (x <= l && x < a.bl)
-            v = a.T[(size_t)l * a.Bp + x] * a.H[((size_t)l * 8 + a.nq[q]) * a.B + x] * a.kappa[(size_t)l * a.NP + q];
+            v = a.T[(size_t)l * a.Bp + x] * a.H[((size_t)l * a.hn + a.nq[q]) * a.B + x] * a.kappa[(size_t)l * a.NP + q];
         a.out[i] = v;
     }
 }
@@ -1396,8 +1397,8 @@ static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 
 static int g_lwalk_variant = 0, g_mwalk_variant = 0;
 
-int lwalk_tile_m(int) { return LW_W * 4; }  // S = 4 pairs per thread in every variant
-int mwalk_tile_m(int) { return MW_W * (g_mwalk_variant == 1 ? 8 : 4); }
+int lwalk_tile_m(int NP) { return LW_W * (NP > 4 ? 2 : 4); }  // pairs per thread: 4, or 2 for N > 8
+int mwalk_tile_m(int NP) { return MW_W * (g_mwalk_variant == 1 && NP <= 4 ? 8 : 4); }
 
 void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t)
 {
@@ -1440,8 +1441,13 @@ static int launch_lwalk_s(const LwalkArgs &a, cudaStream_t s)
     case 2: return launch_lwalk_np<2, S, MINB>(a, s);
     case 3: return launch_lwalk_np<3, S, MINB>(a, s);
     case 4: return launch_lwalk_np<4, S, MINB>(a, s);
+    // N > 8: two pairs per thread keep the accumulators in registers
+    case 5: return launch_lwalk_np<5, 2, 0>(a, s);
+    case 6: return launch_lwalk_np<6, 2, 0>(a, s);
+    case 7: return launch_lwalk_np<7, 2, 0>(a, s);
+    case 8: return launch_lwalk_np<8, 2, 0>(a, s);
     }
-    return set_error(S2DWC_ERROR_SIZE_INVALID, "lwalk: unsupported N=%d (N<=8)", a.N);
+    return set_error(S2DWC_ERROR_SIZE_INVALID, "lwalk: unsupported N=%d (N<=%d)", a.N, S2DW_NMAX);
 }
 
 int launch_lwalk(const LwalkArgs &a, cudaStream_t s)
@@ -1496,8 +1502,13 @@ static int launch_mwalk_q(const MwalkArgs &a, cudaStream_t s)
     case 2: return launch_mwalk_np<2, Q, MINB>(a, s);
     case 3: return launch_mwalk_np<3, Q, MINB>(a, s);
     case 4: return launch_mwalk_np<4, Q, MINB>(a, s);
+    // N > 8: no register cap (the G rows of 5-8 n values stay in registers)
+    case 5: return launch_mwalk_np<5, 4, 0>(a, s);
+    case 6: return launch_mwalk_np<6, 4, 0>(a, s);
+    case 7: return launch_mwalk_np<7, 4, 0>(a, s);
+    case 8: return launch_mwalk_np<8, 4, 0>(a, s);
     }
-    return set_error(S2DWC_ERROR_SIZE_INVALID, "mwalk: unsupported N=%d (N<=8)", a.N);
+    return set_error(S2DWC_ERROR_SIZE_INVALID, "mwalk: unsupported N=%d (N<=%d)", a.N, S2DW_NMAX);
 }
 
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
@@ -1537,13 +1548,13 @@ static int launch_fft_t(const CztArgs &a, cudaStream_t s)
     constexpr int E = V * THREADS;
     const int M = a.czt.M, R = E / M;
     const int nhi = (M + 63) / 64;
-    const size_t smem = sizeof(double2) * ((size_t)padix(E) + 1 + nhi + 64 + 32);
+    const size_t smem = sizeof(double2) * ((size_t)padix(E) + 1 + nhi + 64 + S2DW_NPMAX * S2DW_NMAX);  // + ph[q][g]
     static bool attr[64] = {false};
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
         S2DW_CUDA_TRY(cudaFuncSetAttribute(fft_kernel<V, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(double2) * ((size_t)padix(E) + 1 + 128 + 64 + 32))));
+                                           (int)(sizeof(double2) * ((size_t)padix(E) + 1 + 128 + 64 + S2DW_NPMAX * S2DW_NMAX))));
         attr[dev] = true;
     }
     const int grid = (a.rows + R - 1) / R;
@@ -1571,7 +1582,7 @@ template <int MODE, int LGM>
 static int launch_large_t(const CztArgs &a, cudaStream_t s)
 {
     constexpr int M = 1 << LGM;
-    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + 8);
+    const size_t smem = sizeof(double2) * ((size_t)padix(M) + 1 + M / 64 + 64 + S2DW_NMAX);  // + phases ph[g], g < N
     static bool attr[64] = {false};
     int dev = 0;
     S2DW_CUDA_TRY(cudaGetDevice(&dev));

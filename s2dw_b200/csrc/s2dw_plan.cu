@@ -27,7 +27,8 @@ using namespace s2dw;
 struct s2dwc_plan {
     int B = 0, Bp = 0, N = 0, J = 0, device = 0, form = 0, NP = 0;
     double alpha = 0.0;
-    int nq[4] = {0, 0, 0, 0};
+    int nq[S2DW_NPMAX] = {};
+    int hn = 8;  // n rows of H
     int bl_scoeff = 0;
     bool tables_set = false;
     std::vector<int> bl, blo;
@@ -177,21 +178,25 @@ int plan_build(s2dwc_plan *p)
         band_limits(j, B, p->alpha, &p->bl[j], &p->blo[j]);
         p->wav_off[j + 1] = p->wav_off[j] + (long long)(2 * p->bl[j] - 1) * (2 * p->bl[j]) * N;
     }
-    // host tables depend only on B: build once per process
+    // host tables depend only on B and the rows of H (8, or 16 for N > 8):
+    // build once per process
     static std::mutex rec_mu;
     static std::map<int, std::shared_ptr<RecTables>> rec_cache;
     std::shared_ptr<RecTables> tp;
+    const int hn = N > 8 ? S2DW_NMAX : 8;
     {
         std::lock_guard<std::mutex> g(rec_mu);
-        auto it = rec_cache.find(B);
+        const int key = B * 64 + hn;
+        auto it = rec_cache.find(key);
         if (it == rec_cache.end()) {
             tp = std::make_shared<RecTables>();
-            build_rec_tables(B, *tp);
-            rec_cache[B] = tp;
+            build_rec_tables(B, hn, *tp);
+            rec_cache[key] = tp;
         } else {
             tp = it->second;
         }
     }
+    p->hn = hn;
     const RecTables &t = *tp;
     // row-padded copies (stride Bp) of the tables read by 32-wide tiles
     const int Bp = (B + 31) / 32 * 32;
@@ -354,8 +359,8 @@ std::map<std::tuple<int, int, int, int, long long, int>, std::unique_ptr<s2dwc_p
 int validate_sizes(int B, int N, double alpha, int J)
 {
     if (B < 2) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d must be >= 2", B);
-    if (N < 1 || N > 8)
-        return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d unsupported (1 <= N <= 8)", N);
+    if (N < 1 || N > S2DW_NMAX)
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d unsupported (1 <= N <= %d)", N, S2DW_NMAX);
     if (N > B) return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d exceeds B=%d", N, B);
     if (!(alpha > 1.0)) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha=%g must exceed 1", alpha);
     if (B > 2048) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d exceeds the supported 2048", B);
@@ -1106,6 +1111,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     if (st) return st;
     if (form != S2DWC_FORM_FP64 && form != S2DWC_FORM_SPLIT)
         return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
+    if (form == S2DWC_FORM_SPLIT && N > 8)
+        return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d: the split form supports N <= 8", N);
     int ndev = 0;
     S2DW_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev)
@@ -1217,6 +1224,7 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
         g.blo = p->blo[j];
         std::memcpy(g.nq, p->nq, sizeof(g.nq));
         g.H = p->H;
+        g.hn = p->hn;
         g.T = p->Om;
         g.kappa = p->kappaA + (size_t)j * B * NP;
         g.stride = p->ga_stride[j];

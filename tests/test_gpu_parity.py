@@ -263,3 +263,43 @@ def test_general_slm_device_plan_and_split_rejection():
         sp.analysis_batch(d_flm.reshape(1, B, B), w.reshape(1, -1), sc.reshape(1, -1))
     assert e.value.code == 10
     sp.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha", [(32, 12, 2.0), (24, 16, 2.0), (40, 9, 2.5), (64, 10, 3.0)])
+def test_large_n_matches_oracle(B, N, alpha):
+    """Azimuthal band limits 8 < N <= 16 (FP64 form): analysis and synthesis
+    against the oracle, reconstruction, and a general complex Slm."""
+    t = transform_setup(B, N, alpha)
+    flm = gaussian_flm(B, seed=N)
+    for S in (t["Slm"], _general_slm(B, N, seed=N)):
+        a = (t["K_gamma"], S, t["J"], B, N, t["bl_scoeff"], alpha)
+        s = (t["K_gamma"], t["Phi2"], S, t["J"], B, N, t["bl_scoeff"], alpha)
+        wav, sc = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+        wav_ref, sc_ref = O.analysis_dynamic(flm, *a)
+        for j, (w, r) in enumerate(zip(wav, wav_ref)):
+            if np.abs(r).max() > 0:
+                assert _rel(w, r) <= TOL, f"scale {j}: rel err {_rel(w, r):.3e}"
+        f = core.s2dw_core_synthesis_wav2flm_dynamic(list(wav_ref), sc_ref, *s)
+        f_ref = O.synthesis_dynamic(wav_ref, sc_ref, *s)
+        assert _rel(f, f_ref) <= TOL, f"synthesis rel err {_rel(f, f_ref):.3e}"
+    a = (t["K_gamma"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
+    s = (t["K_gamma"], t["Phi2"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
+    wav, sc = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+    f = core.s2dw_core_synthesis_wav2flm_dynamic(wav, sc, *s)
+    assert np.abs(f - flm).max() <= RECON_TOL
+
+
+@pytest.mark.gpu
+def test_n_limits():
+    """N up to 16 in the FP64 form, up to 8 in the split form."""
+    from s2dw_b200._lib import S2DWError
+    from s2dw_b200.device import Plan
+
+    with pytest.raises(S2DWError) as e:
+        Plan(64, 17, 2.0, 2)
+    assert e.value.code == 8
+    with pytest.raises(S2DWError) as e:
+        Plan(64, 12, 2.0, 2, form=Plan.SPLIT)
+    assert e.value.code == 8
+    Plan(64, 16, 2.0, 2).close()

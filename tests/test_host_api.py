@@ -115,7 +115,7 @@ def test_wav_scale_sizes():
 
 
 def test_invalid_sizes_for_transforms_reported_before_any_device_work():
-    B, N, alpha = 64, 9, 2.0  # N > 8 is outside the supported range
+    B, N, alpha = 64, 17, 2.0  # N > 16 is outside the supported range
     J = core.s2dw_core_comp_Jmax(B, alpha)
     K, P, bs = core.s2dw_core_init_kernels(J, B, alpha)
     S = np.zeros((B, N), dtype=np.complex128, order="F")
