@@ -30,6 +30,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "B=1024 N=4 analysis+synthesis pairs/s at recon err<=1e-10"
+
+
+def _hbm_gbs():
+    """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json,
+    hbm_gbs), else the earlier measured fallback of 6650 GB/s."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+HBM_GBS = _hbm_gbs()
 UNIT = "pairs/s"
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
@@ -556,8 +569,14 @@ def main():
                     "avg_launch_ms": per_launch_ms}
     kernel_tflops = {k: (algo[k] * ksteps / (v[1] / 1e3) / 1e12 if k in algo and v[1] > 0 else None)
                      for k, v in kt.items()}
+    # achieved DRAM bandwidth per kind: the ncu traffic per launch of this
+    # workload (when known) times the launches, over the CUDA-event time
+    trf = NCU_TRAFFIC.get((B, N, float(alpha)), {})
+    kernel_gbs = {k: (trf[k] * v[0] / (v[1] / 1e3) / 1e9 if k in trf and v[1] > 0 else None) for k, v in kt.items()}
     kernel_ms = {k: {"launches_per_step": v[0] / ksteps, "ms_per_step": v[1] / ksteps,
-                     "tflops": kernel_tflops[k]} for k, v in kt.items()}
+                     "tflops": kernel_tflops[k], "dram_gbs": kernel_gbs[k],
+                     "dram_frac_of_hbm": (kernel_gbs[k] / HBM_GBS if kernel_gbs[k] else None)}
+                 for k, v in kt.items()}
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
