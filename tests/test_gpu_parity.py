@@ -303,3 +303,33 @@ def test_n_limits():
         Plan(64, 12, 2.0, 2, form=Plan.SPLIT)
     assert e.value.code == 8
     Plan(64, 16, 2.0, 2).close()
+
+
+@pytest.mark.gpu
+def test_host_api_staged_copies_multichunk():
+    """Pageable caller arrays go through the plan's page-locked staging
+    buffers in 32 MB chunks: at B=512 the dynamic and the static layouts span
+    several chunks and agree with each other and with a page-locked run."""
+    import torch
+
+    B, N, alpha = 512, 3, 2.0
+    t = transform_setup(B, N, alpha)
+    J, bs = t["J"], t["bl_scoeff"]
+    flm = gaussian_flm(B, seed=21)
+    a = (t["K_gamma"], t["Slm"], J, B, N, bs, alpha)
+    s = (t["K_gamma"], t["Phi2"], t["Slm"], J, B, N, bs, alpha)
+    wav_d, sc_d = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+    wav_s, sc_s = core.s2dw_core_analysis_flm2wav(flm, *a)
+    for j, w in enumerate(wav_d):
+        np.testing.assert_array_equal(wav_s[j, :w.shape[0], :w.shape[1], :], w)
+    pinned = []
+    for w in wav_d:
+        buf = torch.empty(w.size, dtype=torch.float64, pin_memory=True).numpy().reshape(w.shape, order="F")
+        buf[...] = w
+        pinned.append(buf)
+    f_pageable = core.s2dw_core_synthesis_wav2flm_dynamic([w.copy(order="F") for w in wav_d], sc_d, *s)
+    f_pinned = core.s2dw_core_synthesis_wav2flm_dynamic(pinned, sc_d, *s)
+    f_static = core.s2dw_core_synthesis_wav2flm(wav_s, sc_s, *s)
+    np.testing.assert_array_equal(f_pageable, f_pinned)
+    np.testing.assert_array_equal(f_static, f_pinned)
+    assert np.abs(f_pinned - flm).max() <= RECON_TOL
