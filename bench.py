@@ -622,6 +622,30 @@ def main():
                "d2h_bytes_per_step": wav_bytes + 16 * bs * bs + 16 * B * B,
                "recon_err": e2e_recon,
                "api": "s2dwc_analysis_flm2wav_dynamic + s2dwc_synthesis_wav2flm_dynamic, pinned host buffers"}
+        # the same with ordinary (pageable) arrays, as Fortran callers pass them
+        pg = [np.zeros(core.wav_scale_shape(j, B, N, alpha), order="F") for j in range(J + 1)]
+        wptr = (dp * (J + 1))(*[w.ctypes.data_as(dp) for w in pg])
+        flm_p = [np.asfortranarray(f) for f in flms]
+        out_p = np.zeros((B, B), dtype=np.complex128, order="F")
+
+        def e2e_step_p(i):
+            check(L.s2dwc_analysis_flm2wav_dynamic(wptr, sc_h.ctypes.data_as(dp), flm_p[i % nring].ctypes.data_as(dp),
+                                                   K.ctypes.data_as(dp), S.ctypes.data_as(dp), J, B, N, bs, alpha))
+            check(L.s2dwc_synthesis_wav2flm_dynamic(out_p.ctypes.data_as(dp), wptr, sc_h.ctypes.data_as(dp),
+                                                    K.ctypes.data_as(dp), P.ctypes.data_as(dp), S.ctypes.data_as(dp),
+                                                    J, B, N, bs, alpha))
+
+        for i in range(2):
+            e2e_step_p(i)
+        barrier(world)
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            e2e_step_p(i)
+        tp = max_over_ranks(time.perf_counter() - t0, world)
+        e2e["pageable"] = {"value": args.e2e_steps * world / tp, "unit": UNIT,
+                           "recon_err": float(np.abs(out_p - flms[(args.e2e_steps - 1) % nring]).max()),
+                           "api": "same entry points, pageable numpy arrays (staged through page-locked buffers)"}
+        del pg
 
     graphs.clear()
     serving = None
