@@ -622,6 +622,26 @@ def main():
                "d2h_bytes_per_step": wav_bytes + 16 * bs * bs + 16 * B * B,
                "recon_err": e2e_recon,
                "api": "s2dwc_analysis_flm2wav_dynamic + s2dwc_synthesis_wav2flm_dynamic, pinned host buffers"}
+        # PCIe floor: plain page-locked copies of the same bytes, one direction
+        # at a time as a pair of calls moves them (the analysis output leaves
+        # before the synthesis input arrives)
+        nb = wav_bytes // 8
+        hbuf = torch.empty(nb, dtype=torch.float64, pin_memory=True)
+        dbuf = torch.empty(nb, dtype=torch.float64, device=f"cuda:{local}")
+        rates = {}
+        for name, dst, src in (("h2d", dbuf, hbuf), ("d2h", hbuf, dbuf)):
+            dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(4):
+                dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            rates[name] = 4 * wav_bytes / (time.perf_counter() - t0) / 1e9
+        floor_s = e2e["h2d_bytes_per_step"] / (rates["h2d"] * 1e9) + e2e["d2h_bytes_per_step"] / (rates["d2h"] * 1e9)
+        e2e["copy_floor"] = {"h2d_gbs": rates["h2d"], "d2h_gbs": rates["d2h"], "pairs_per_s": 1.0 / floor_s,
+                             "frac": e2e["value"] / world / (1.0 / floor_s),
+                             "what": "pinned cudaMemcpy of the step's bytes, no kernels: the bound of e2e"}
+        del hbuf, dbuf
         # the same with ordinary (pageable) arrays, as Fortran callers pass them
         pg = [np.zeros(core.wav_scale_shape(j, B, N, alpha), order="F") for j in range(J + 1)]
         wptr = (dp * (J + 1))(*[w.ctypes.data_as(dp) for w in pg])

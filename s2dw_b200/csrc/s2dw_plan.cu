@@ -70,6 +70,15 @@ struct s2dwc_plan {
     // two page-locked staging buffers for pageable caller arrays (first use)
     char *stage[2] = {nullptr, nullptr};
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    // host-buffer entry points: the caller's tables last folded in (compared
+    // by content, so that repeated calls with the same K_gamma and Slm keep
+    // the device tables), a copy stream, and per-scale events that order the
+    // copies against the scales' kernels (created on first use)
+    std::vector<double> hc_K, hc_S, hc_Phi2;
+    int hc_bls = -1;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_host = nullptr;
+    std::vector<cudaEvent_t> ev_done, ev_copy;
     long long ws_bytes = 0;
     // optional per-kernel CUDA-event timing: (kind, start, stop) per launch
     bool timing = false;
@@ -124,6 +133,10 @@ struct s2dwc_plan {
         for (auto st : streams) cudaStreamDestroy(st);
         for (auto ev : ev_join) cudaEventDestroy(ev);
         if (ev_fork) cudaEventDestroy(ev_fork);
+        for (auto ev : ev_done) cudaEventDestroy(ev);
+        for (auto ev : ev_copy) cudaEventDestroy(ev);
+        if (ev_host) cudaEventDestroy(ev_host);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         for (void *p : allocs) cudaFree(p);
         for (int i = 0; i < 2; i++) {
             if (stage[i]) cudaFreeHost(stage[i]);
@@ -439,8 +452,12 @@ struct KernelTimer {
 // overlap each scale's host<->device copy with the other scales' kernels.
 using ScaleHook = std::function<int(int, cudaStream_t)>;
 
+// full_band_serial (host-buffer entry points): the scales of the largest band
+// limit, which hold most of the coefficients, run one after another, the
+// last scale first, so that the first one's device-to-host copy overlaps the
+// next one's kernels instead of all of them finishing together at the end.
 int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 *d_flm, cudaStream_t s,
-                 const ScaleHook &after = ScaleHook())
+                 const ScaleHook &after = ScaleHook(), bool full_band_serial = false)
 {
     int st;
     {
@@ -448,12 +465,17 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         if ((st = launch_fprep(p->Fw, d_flm, p->Om, p->B, p->Bp, s))) return st;
     }
     S2DW_CUDA_TRY(cudaEventRecord(p->ev_fork, s));
-    for (int j = 0; j <= p->J; j++) {
+    const bool serial = full_band_serial && !p->timing && (int)p->ev_done.size() == p->J + 1;
+    int prev_full = -1;
+    for (int jj = 0; jj <= p->J; jj++) {
+        const int j = serial ? p->J - jj : jj;
         // per-kernel timing runs every launch on the caller's stream so that
         // each event pair brackets one kernel running alone
         cudaStream_t sj = p->timing ? s : p->streams[j];
         if (!p->timing) S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_fork, 0));
         const int bl = p->bl[j];
+        const bool full = serial && bl == p->bl[p->J];
+        if (full && prev_full >= 0) S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_done[prev_full], 0));
         double2 *Tg = p->wsC + p->offC[j], *Tb = p->wsA + p->offA[j];
         LwalkArgs la{};
         la.B = p->B;
@@ -507,6 +529,10 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         {
             KernelTimer kt(p, S2DWC_KIND_ANA_ALPHA, sj);
             if ((st = launch_czt(ca, sj))) return st;
+        }
+        if (full) {
+            S2DW_CUDA_TRY(cudaEventRecord(p->ev_done[j], sj));
+            prev_full = j;
         }
         if (after && (st = after(j, sj))) return st;
         if (!p->timing) S2DW_CUDA_TRY(cudaEventRecord(p->ev_join[j], sj));
@@ -1557,15 +1583,62 @@ struct HostCallBuffers {
     double2 *flm = nullptr, *sc = nullptr;
 };
 
+// Folds the caller's tables into the cached plan unless they equal, byte for
+// byte, the ones folded last: callers pass the same K_gamma and Slm on every
+// call, and refolding them costs 2(J+1) table kernels and a device
+// synchronisation per call.  Phi2 (synthesis only) is compared and uploaded
+// on its own; the analysis passes none and leaves the plan's copy as is.
+static int host_fold_tables(s2dwc_plan *p, const double *K_gamma, const double *Phi2, const double *Slm,
+                            int bl_scoeff)
+{
+    const size_t nK = (size_t)(p->J + 1) * p->B, nS = 2 * (size_t)p->B * p->N, nP = (size_t)p->B;
+    const bool same = p->tables_set && p->hc_bls == bl_scoeff && p->hc_K.size() == nK && p->hc_S.size() == nS &&
+                      std::memcmp(p->hc_K.data(), K_gamma, nK * sizeof(double)) == 0 &&
+                      std::memcmp(p->hc_S.data(), Slm, nS * sizeof(double)) == 0;
+    if (!same) {
+        p->hc_K.clear();
+        p->hc_S.clear();
+        p->hc_Phi2.clear();
+        int st = s2dwc_plan_set_tables(p, K_gamma, Phi2, Slm, bl_scoeff);
+        if (st) return st;
+        p->hc_K.assign(K_gamma, K_gamma + nK);
+        p->hc_S.assign(Slm, Slm + nS);
+        if (Phi2) p->hc_Phi2.assign(Phi2, Phi2 + nP);
+        p->hc_bls = bl_scoeff;
+        return S2DWC_OK;
+    }
+    if (Phi2 && (p->hc_Phi2.size() != nP || std::memcmp(p->hc_Phi2.data(), Phi2, nP * sizeof(double)) != 0)) {
+        DeviceGuard dg(p->device);
+        p->hc_Phi2.clear();
+        S2DW_CUDA_TRY(cudaMemcpy(p->Phi2, Phi2, nP * sizeof(double), cudaMemcpyHostToDevice));
+        p->hc_Phi2.assign(Phi2, Phi2 + nP);
+    }
+    return S2DWC_OK;
+}
+
+// Looks up the cached plan of (B, N, alpha, J), takes its lock for the rest
+// of the call, folds the tables and returns the plan's host-call buffers.
 static int host_prepare(int B, int N, double alpha, int J, int bl_scoeff, const double *K_gamma,
-                        const double *Phi2, const double *Slm, s2dwc_plan **pp, HostCallBuffers &hb)
+                        const double *Phi2, const double *Slm, s2dwc_plan **pp, HostCallBuffers &hb,
+                        std::unique_lock<std::mutex> &lk)
 {
     int st = validate_sizes(B, N, alpha, J);
     if (st) return st;
     if ((st = get_cached_plan(B, N, alpha, J, pp))) return st;
     s2dwc_plan *p = *pp;
-    if ((st = s2dwc_plan_set_tables(p, K_gamma, Phi2, Slm, bl_scoeff))) return st;
+    lk = std::unique_lock<std::mutex>(p->mu);
+    if ((st = host_fold_tables(p, K_gamma, Phi2, Slm, bl_scoeff))) return st;
     DeviceGuard dg(p->device);
+    if (!p->copy_stream) {
+        p->ev_done.assign(J + 1, nullptr);
+        p->ev_copy.assign(J + 1, nullptr);
+        for (int j = 0; j <= J; j++) {
+            S2DW_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_done[j], cudaEventDisableTiming));
+            S2DW_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_copy[j], cudaEventDisableTiming));
+        }
+        S2DW_CUDA_TRY(cudaEventCreateWithFlags(&p->ev_host, cudaEventDisableTiming));
+        S2DW_CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    }
     if (!p->hbWav) {
         if ((st = dev_alloc(p, &p->hbWav, (size_t)std::max(1LL, p->wav_off[J + 1]))) ||
             (st = dev_alloc(p, &p->hbFlm, (size_t)B * B)))
@@ -1670,13 +1743,14 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
         return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null pointer");
     s2dwc_plan *p = nullptr;
     HostCallBuffers hb;
-    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, nullptr, Slm, &p, hb);
+    std::unique_lock<std::mutex> lk;
+    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, nullptr, Slm, &p, hb, lk);
     if (st) return st;
-    std::lock_guard<std::mutex> g(p->mu);
     DeviceGuard dg(p->device);
     S2DW_CUDA_TRY(cudaMemcpy(hb.flm, flm, sizeof(double2) * (size_t)B * B, cudaMemcpyHostToDevice));
     // pinned per-scale outputs: each scale's device-to-host copy follows its
-    // kernels on its stream and overlaps the other scales
+    // kernels on its stream and overlaps the other scales' kernels, the
+    // full-band scales one after another
     const bool overlap = wav_scales && all_pinned(reinterpret_cast<const void *const *>(wav_scales), J + 1);
     ScaleHook copy_out;
     if (overlap)
@@ -1686,7 +1760,12 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
                                           cudaMemcpyDeviceToHost, sj));
             return S2DWC_OK;
         };
-    if ((st = run_analysis(p, hb.wav, hb.sc, hb.flm, 0, copy_out))) return st;
+    if ((st = run_analysis(p, hb.wav, hb.sc, hb.flm, 0, copy_out, overlap))) {
+        // no copy into the caller's arrays may outlive the call
+        if (overlap)
+            for (int j = 0; j <= J; j++) cudaStreamSynchronize(p->streams[j]);
+        return st;
+    }
     if (bl_scoeff > 0)
         S2DW_CUDA_TRY(cudaMemcpy(scoeff, hb.sc, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
                                  cudaMemcpyDeviceToHost));
@@ -1747,19 +1826,27 @@ static int synthesis_host(double *flm, const double *wav_static, const double *c
         return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null pointer");
     s2dwc_plan *p = nullptr;
     HostCallBuffers hb;
-    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, Phi2, Slm, &p, hb);
+    std::unique_lock<std::mutex> lk;
+    int st = host_prepare(B, N, alpha, J, bl_scoeff, K_gamma, Phi2, Slm, &p, hb, lk);
     if (st) return st;
-    std::lock_guard<std::mutex> g(p->mu);
     DeviceGuard dg(p->device);
-    // pinned per-scale inputs: each scale's host-to-device copy precedes its
-    // kernels on its stream and overlaps the other scales
+    // pinned per-scale inputs: one copy stream brings the scales in, the last
+    // (largest) first, and each scale's kernels wait for their own copy only,
+    // so the largest scales' kernels overlap the remaining copies and the
+    // kernels left after the last copy are the small scales'
     const bool overlap = wav_scales && all_pinned(reinterpret_cast<const void *const *>(wav_scales), J + 1);
     ScaleHook copy_in;
     if (overlap) {
-        copy_in = [&](int j, cudaStream_t sj) -> int {
+        S2DW_CUDA_TRY(cudaEventRecord(p->ev_host, 0));
+        S2DW_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->ev_host, 0));
+        for (int j = J; j >= 0; j--) {
             S2DW_CUDA_TRY(cudaMemcpyAsync(hb.wav + p->wav_off[j], wav_scales[j],
                                           sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j]),
-                                          cudaMemcpyHostToDevice, sj));
+                                          cudaMemcpyHostToDevice, p->copy_stream));
+            S2DW_CUDA_TRY(cudaEventRecord(p->ev_copy[j], p->copy_stream));
+        }
+        copy_in = [&](int j, cudaStream_t sj) -> int {
+            S2DW_CUDA_TRY(cudaStreamWaitEvent(sj, p->ev_copy[j], 0));
             return S2DWC_OK;
         };
     } else if (wav_scales) {
@@ -1790,7 +1877,10 @@ static int synthesis_host(double *flm, const double *wav_static, const double *c
     if (bl_scoeff > 0)
         S2DW_CUDA_TRY(cudaMemcpy(hb.sc, scoeff, sizeof(double2) * (size_t)bl_scoeff * bl_scoeff,
                                  cudaMemcpyHostToDevice));
-    if ((st = run_synthesis(p, hb.flm, hb.wav, hb.sc, 0, copy_in))) return st;
+    if ((st = run_synthesis(p, hb.flm, hb.wav, hb.sc, 0, copy_in))) {
+        if (overlap) cudaStreamSynchronize(p->copy_stream);  // no read of the caller's arrays outlives the call
+        return st;
+    }
     S2DW_CUDA_TRY(cudaMemcpy(flm, hb.flm, sizeof(double2) * (size_t)B * B, cudaMemcpyDeviceToHost));
     return S2DWC_OK;
 }

@@ -333,3 +333,63 @@ def test_host_api_staged_copies_multichunk():
     np.testing.assert_array_equal(f_pageable, f_pinned)
     np.testing.assert_array_equal(f_static, f_pinned)
     assert np.abs(f_pinned - flm).max() <= RECON_TOL
+
+
+@pytest.mark.gpu
+def test_host_api_table_changes_take_effect():
+    """The host entry points keep the folded tables while the caller passes the
+    same K_gamma, Slm and bl_scoeff; a change of any of them (in place, through
+    the same array) or of Phi2 gives the result of the new tables, and going
+    back gives the first result bit for bit."""
+    B, N, alpha = 64, 3, 2.0
+    t = transform_setup(B, N, alpha)
+    J, bs = t["J"], t["bl_scoeff"]
+    flm = gaussian_flm(B, seed=31)
+    flm[0, 0] = 0.7  # a nonzero scaling coefficient, so that Phi2 enters the synthesis
+    K = np.asfortranarray(t["K_gamma"].copy())
+    S = np.asfortranarray(t["Slm"].copy())
+    P = t["Phi2"].copy()
+
+    def ana(bsv=bs):
+        return core.s2dw_core_analysis_flm2wav_dynamic(flm, K, S, J, B, N, bsv, alpha)
+
+    def syn(w, sc, bsv=bs):
+        return core.s2dw_core_synthesis_wav2flm_dynamic([x.copy(order="F") for x in w], sc, K, P, S, J, B, N,
+                                                        bsv, alpha)
+
+    wA, scA = ana()
+    fA = syn(wA, scA)
+    K0 = K.copy()
+    K[...] = K0 * 1.25
+    wK, _ = ana()
+    assert any(not np.array_equal(a, b) for a, b in zip(wA, wK))
+    K[...] = K0
+    S0 = S.copy()
+    S[...] = S0 * (0.5 + 0.25j)
+    wS, _ = ana()
+    assert any(not np.array_equal(a, b) for a, b in zip(wA, wS))
+    S[...] = S0
+    w2, sc2 = ana()
+    for a, b in zip(wA, w2):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(scA, sc2)
+    # Phi2 alone
+    P[...] = t["Phi2"] * 2.0
+    fP = syn(wA, scA)
+    assert not np.array_equal(fA, fP)
+    P[...] = t["Phi2"]
+    np.testing.assert_array_equal(syn(wA, scA), fA)
+    # K changed in place between two syntheses
+    K[...] = K0 * 1.25
+    fK = syn(wA, scA)
+    assert not np.array_equal(fA, fK)
+    K[...] = K0
+    np.testing.assert_array_equal(syn(wA, scA), fA)
+    # bl_scoeff
+    wb, scb = ana(bs + 1)
+    assert scb.shape == (bs + 1, bs + 1)
+    np.testing.assert_array_equal(scb[:bs, :bs], scA)
+    w3, sc3 = ana()
+    for a, b in zip(wA, w3):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(scA, sc3)
