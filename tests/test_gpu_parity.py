@@ -308,11 +308,13 @@ def test_n_limits():
 @pytest.mark.gpu
 def test_host_api_staged_copies_multichunk():
     """Pageable caller arrays go through the plan's page-locked staging
-    buffers in 32 MB chunks: at B=512 the dynamic and the static layouts span
-    several chunks and agree with each other and with a page-locked run."""
+    buffers in 32 MB chunks, a scale at a time and overlapped with the other
+    scales' kernels: at B=512, N=5 each full-band scale (42 MB) spans two
+    chunks; the dynamic and the static layouts agree with each other and with
+    a page-locked run."""
     import torch
 
-    B, N, alpha = 512, 3, 2.0
+    B, N, alpha = 512, 5, 2.0
     t = transform_setup(B, N, alpha)
     J, bs = t["J"], t["bl_scoeff"]
     flm = gaussian_flm(B, seed=21)
