@@ -155,6 +155,25 @@ def contraction_flops_per_scale(B, N, alpha, J):
     return ana, syn
 
 
+def pair_roofline(B, N, alpha, J, t_ms, fp64_peak_tflops):
+    """Whole-pair roofline: t_min = max(F / P_FP64, Q / BW_HBM) with F the
+    contraction flops of an analysis+synthesis pair (4 per complex-by-real MAC)
+    and Q its compulsory HBM bytes (the wavelet array written then read, flm
+    read then written: 2*8*samples + 2*16*B(B+1)/2); frac = t_min / t."""
+    from s2dw_b200 import core
+
+    ana_f, syn_f = contraction_flops_per_scale(B, N, alpha, J)
+    F = sum(ana_f) + sum(syn_f)
+    samples = sum(int(np.prod(core.wav_scale_shape(j, B, N, alpha))) for j in range(J + 1))
+    Q = 2 * 8 * samples + 2 * 16 * B * (B + 1) / 2
+    t_f = F / (fp64_peak_tflops * 1e12) * 1e3
+    t_q = Q / (HBM_GBS * 1e9) * 1e3
+    t_min = max(t_f, t_q)
+    return {"flops": F, "bytes": Q, "t_flops_ms": t_f, "t_hbm_ms": t_q, "t_min_ms": t_min, "t_ms": t_ms,
+            "frac": t_min / t_ms, "bound": "fp64" if t_f >= t_q else "hbm",
+            "peaks": f"FP64 {fp64_peak_tflops:.1f} TFLOP/s (measured DGEMM), HBM {HBM_GBS:.0f} GB/s (measured copy)"}
+
+
 def _serve(srv, reqs, rate=None):
     """Warm-up (one request per configuration and kind), then the whole
     stream at once (saturation throughput), then Poisson arrivals at `rate`
@@ -566,7 +585,8 @@ def main():
                     "traffic_unit": "bytes per launch (ncu, mean over a pair's launches)",
                     "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (MEASURED_PEAKS.json has no fp64 entry)",
                     "flops_per_pair": algo[dom[0]], "launches_per_pair": launches_per_pair,
-                    "avg_launch_ms": per_launch_ms}
+                    "avg_launch_ms": per_launch_ms,
+                    "pair": pair_roofline(B, N, alpha, J, 1e3 * elapsed / args.steps, fp64_peak)}
     kernel_tflops = {k: (algo[k] * ksteps / (v[1] / 1e3) / 1e12 if k in algo and v[1] > 0 else None)
                      for k, v in kt.items()}
     # achieved DRAM bandwidth per kind: the ncu traffic per launch of this
@@ -701,6 +721,7 @@ def main():
     if args.split_maps > 0:
         try:
             split = split_stats(B, N, alpha, J, args.split_maps)
+            split["pair_roofline"] = pair_roofline(B, N, alpha, J, 1e3 / split["value"], fp64_peak)
         except Exception as ex:
             split = {"error": str(ex)[:300]}
 
