@@ -50,6 +50,9 @@ int positive_nset(int N, int *nq);
 // so at most S2DW_NPMAX values n >= 0 with N + n odd.
 constexpr int S2DW_NMAX = 16;
 constexpr int S2DW_NPMAX = S2DW_NMAX / 2;
+// Largest scale index J (scales j = 0..J): per-scale arrays passed to kernels
+// by value are sized by it (J+1 entries, under 2.2 KB of kernel arguments).
+constexpr int S2DW_JMAX = 127;
 
 struct RecTables {
     int B = 0, HN = 8;
@@ -154,8 +157,8 @@ int mwalk_tile_m(int NP);  // m values per mwalk CTA tile
 // s2dw_core_mod.f90:1228-1253 in scale order followed by :1258-1261.
 struct CombineArgs {
     int B, J, bs;
-    int bl[16], blo[16];
-    long long off[16];   // offset of part_j in `parts` (complex values)
+    int bl[S2DW_JMAX + 1], blo[S2DW_JMAX + 1];
+    long long off[S2DW_JMAX + 1];  // offset of part_j in `parts` (complex values)
     const double2 *parts;
     const double2 *scoeff;
     const double *Phi2;
@@ -283,7 +286,7 @@ constexpr int STAT_P = 64;  // blocks per (map, scale) in the reduction passes
 struct StatArgs {
     int J, nmaps;
     long long wtot;            // doubles per map in the packed layout
-    long long off[17];         // scale offsets (J+2 entries)
+    long long off[S2DW_JMAX + 2];  // scale offsets (J+2 entries)
     const double *wav;         // map k at wav + k*wtot
     const double *mask;        // packed layout of one map, or null
     double *part;              // nmaps*(J+1)*STAT_P*6 partial sums

@@ -384,7 +384,7 @@ int validate_sizes(int B, int N, double alpha, int J)
     if (N > B) return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d exceeds B=%d", N, B);
     if (!(alpha > 1.0)) return set_error(S2DWC_ERROR_SIZE_INVALID, "alpha=%g must exceed 1", alpha);
     if (B > 2048) return set_error(S2DWC_ERROR_SIZE_INVALID, "B=%d exceeds the supported 2048", B);
-    if (J > 15) return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d exceeds the supported 15", J);
+    if (J > S2DW_JMAX) return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d exceeds the supported %d", J, S2DW_JMAX);
     if (!params_valid(J, B, alpha, N))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "J=%d invalid for B=%d alpha=%g (1<=J<=%d)", J, B,
                          alpha, comp_jmax(B, alpha));
@@ -1449,7 +1449,7 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
 {
     if (!wav_scales || !mean || !var || !skew || !kur)
         return set_error(S2DWC_ERROR_ARG_INVALID, "stat_moments: null pointer");
-    if (B < 2 || N < 1 || J < 0 || J > 15 || !(alpha > 1.0))
+    if (B < 2 || N < 1 || J < 0 || J > S2DW_JMAX || !(alpha > 1.0))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "stat_moments: B=%d N=%d J=%d alpha=%g", B, N, J, alpha);
     for (int j = 0; j <= J; j++)
         if (!wav_scales[j] || (mask_scales && !mask_scales[j]))
