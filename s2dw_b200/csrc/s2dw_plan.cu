@@ -1824,7 +1824,8 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
         std::vector<HostSeg> segs;
         std::vector<cudaEvent_t> wait;
         for (int j = J; j >= 0; j--) {
-            char *h = wav_scales ? reinterpret_cast<char *>(wav_scales[j]) : reinterpret_cast<char *>(tmp.get() + p->wav_off[j]);
+            char *h = wav_scales ? reinterpret_cast<char *>(wav_scales[j])
+                                 : reinterpret_cast<char *>(tmp.get() + p->wav_off[j]);
             segs.push_back({h, reinterpret_cast<char *>(hb.wav + p->wav_off[j]),
                             sizeof(double) * (size_t)(p->wav_off[j + 1] - p->wav_off[j])});
             wait.push_back(p->ev_copy[j]);
@@ -1843,8 +1844,9 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
                         wav_static[j + J1 * (a + A * (b + BB * g))] = src[a + (size_t)n * (b + 2 * (size_t)bl * g)];
         };
         StagedCopy sc(p, segs, p->copy_stream);
-        if ((st = sc.start()) ||
-            (st = sc.to_host(wait.data(), wav_scales ? std::function<void(size_t)>() : std::function<void(size_t)>(scatter)))) {
+        std::function<void(size_t)> seg_done;
+        if (!wav_scales) seg_done = scatter;
+        if ((st = sc.start()) || (st = sc.to_host(wait.data(), seg_done))) {
             cudaStreamSynchronize(p->copy_stream);
             return st;
         }
