@@ -122,3 +122,55 @@ def test_invalid_sizes_for_transforms_reported_before_any_device_work():
     with pytest.raises(S2DWError) as e:
         core.s2dw_core_analysis_flm2wav_dynamic(np.zeros((B, B), complex), K, S, J, B, N, bs, alpha)
     assert e.value.code == 8
+
+
+def _kgamma_pairwise(J, B, alpha):
+    """K_gamma of s2dw_core_init_kernels (s2dw_core_mod.f90:97-157) with each
+    Simpson level's sum formed pairwise over directly computed sample points
+    (numpy's summation order, the order a parallel reduction takes) instead of
+    the reference's left-to-right sum over accumulated points."""
+    def f(k, bw, lo):
+        t = 2.0 * ((k - lo) / (bw - lo)) - 1.0
+        return np.exp(-2.0 / (1.0 - t * t)) / k
+
+    def simpson(bw, lo, a, b):
+        st = os_ = ost = 0.0
+        for j in range(1, 41):
+            if j == 1:
+                st = 0.5 * (b - a) * (f(a, bw, lo) + f(b, bw, lo))
+            else:
+                it = 1 << (j - 2)
+                dl = (b - a) / it
+                st = 0.5 * (st + (b - a) * np.sum(f(a + (np.arange(it) + 0.5) * dl, bw, lo)) / it)
+            s = (4.0 * st - ost) / 3.0
+            if j > 5 and (abs(s - os_) < 1e-12 * abs(os_) or (s == 0.0 and os_ == 0.0)):
+                return s
+            os_, ost = s, st
+        raise AssertionError("no convergence")
+
+    def snap(x, rnd):
+        ok, y = core.s2dw_core_assimilate_int(x)
+        return y if ok else int(rnd(x))
+
+    phi2 = np.zeros((J + 2, B))
+    for jj in range(J + 2):
+        bw = snap(B / alpha ** (jj - 1), np.ceil)
+        lo = snap(bw / alpha, np.floor)
+        c = simpson(bw, lo, lo + 1e-12, bw - 1e-12)
+        for el in range(B):
+            phi2[jj, el] = 1.0 if el <= lo else 0.0 if el >= bw else simpson(bw, lo, float(el), bw - 1e-12) / c
+    return np.sqrt(np.maximum(phi2[:-1] - phi2[1:], 0.0))
+
+
+@pytest.mark.parametrize("B", [64, 256])
+def test_kernel_tables_need_the_reference_summation_order(B):
+    """Why the kernel tables are built on the host in the reference's order:
+    K_gamma = sqrt(Phi2_{j-1} - Phi2_j), and in each scale's tails the two
+    quadratures nearly cancel, so a reordered sum that changes K_gamma^2 only
+    within the quadrature's own tolerance (TOL_QUAD = 1e-12,
+    s2dw_types_mod.f90:54) moves K_gamma far beyond the 1e-12 parity bar."""
+    J = core.s2dw_core_comp_Jmax(B, 2.0)
+    K, _, _ = core.s2dw_core_init_kernels(J, B, 2.0)
+    Kp = _kgamma_pairwise(J, B, 2.0)
+    assert np.abs(Kp ** 2 - K ** 2).max() <= 1e-12
+    assert np.abs(Kp - K).max() > 1e-10
