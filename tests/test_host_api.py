@@ -33,6 +33,16 @@ def test_library_exports_every_declared_symbol():
     assert os.path.abspath(s2dw_b200.LIB_PATH).startswith(ROOT)
 
 
+def test_ctypes_signatures_match_header_arity():
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "s2dw_cuda.h")).read(), flags=re.S)
+    protos = {m.group(1): m.group(2) for m in
+              re.finditer(r"\b(s2dwc_\w+)\s*\(([^;]*?)\)\s*;", txt, re.S)}
+    assert len(protos) >= 25
+    for name, params in protos.items():
+        n = 0 if params.strip() in ("", "void") else len(params.split(","))
+        assert len(SIGNATURES[name][1]) == n, f"{name}: ctypes has {len(SIGNATURES[name][1])} arguments, C has {n}"
+
+
 @pytest.mark.parametrize("B,alpha", [(64, 2.0), (1024, 2.0), (256, 3.0), (100, 2.5), (2048, 2.0), (7, 2.0)])
 def test_kernel_tables_bit_identical_to_oracle(B, alpha):
     J = core.s2dw_core_comp_Jmax(B, alpha)
