@@ -22,9 +22,14 @@
  * for s2dwc_last_error_message().
  *
  * Host-buffer entry points are synchronous and allocate their device
- * workspace through a per-(B,N,alpha,J,device) plan cache.  Device entry
- * points (s2dwc_plan_*) take device pointers and a CUDA stream and never
- * synchronise.
+ * workspace through a per-(B,N,alpha,J,device) plan cache.  The cached plan
+ * keeps the tables folded from the caller's K_gamma, Slm and bl_scoeff while
+ * later calls pass the same values (compared by content, so arrays changed
+ * in place are picked up).  Their host<->device copies overlap the kernels a
+ * scale at a time; page-locked per-scale arrays (cudaHostAlloc) copy at the
+ * full PCIe rate, other arrays go through page-locked staging buffers of the
+ * plan.  Device entry points (s2dwc_plan_*) take device pointers and a CUDA
+ * stream and never synchronise.
  */
 #ifndef S2DW_CUDA_H
 #define S2DW_CUDA_H
