@@ -163,6 +163,21 @@ typedef struct s2dwc_plan s2dwc_plan;
 int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int form, int device);
 int s2dwc_plan_destroy(s2dwc_plan *plan);
 
+/* Device bytes s2dwc_plan_create would allocate for (B, N, alpha, J, form),
+ * computed on the host without touching a device (the split form's batch
+ * workspaces, sized per batch later, are not included). */
+int s2dwc_plan_footprint(int B, int N, double alpha, int J, int form, long long *bytes);
+
+/* Limits the device memory one plan may hold to `bytes` (0: no limit, the
+ * default; process-wide).  A plan whose footprint exceeds it is refused by
+ * s2dwc_plan_create before any device call, and any later workspace growth
+ * beyond it (split-form batches, host-buffer entry points) fails, both with
+ * S2DWC_ERROR_MEM_ALLOC_FAIL -- the status the reference gives when an
+ * allocate fails (src/mod/s2dw_core_mod.f90:384-385, :598-602).  The
+ * host-buffer entry points create their plans through s2dwc_plan_create and
+ * obey the same limit. */
+int s2dwc_set_plan_memory_limit(long long bytes);
+
 /* Uploads the caller's kernel tables (host pointers, reference layouts).
  * Phi2 may be NULL for analysis-only use.  Any complex Slm is accepted; one
  * not of the form s2dw_core_init_directionality produces (S/eta real, eta = 1
@@ -250,11 +265,16 @@ int s2dwc_plan_check(s2dwc_plan *plan);
  * would synchronise the device and stall other streams.
  *  - Limit: the plan must need at most S2DWC_NOALLOC_SCRATCH_BYTES of scratch
  *    (16 (B B_pad + 3 N B^2) bytes, B_pad = B rounded up to a multiple of
- *    32, plus alignment): any B <= 256 with N <= 8, or B = 512 with N <= 2.  Larger plans are
- *    rejected with S2DWC_ERROR_SIZE_INVALID.
+ *    32, plus alignment): any B <= 256 with N <= 10, or B <= 512 with N <= 2.
+ *    Larger plans are rejected with S2DWC_ERROR_SIZE_INVALID.
+ *  - Form: the FP64 form only.  A plan created with S2DWC_FORM_SPLIT is
+ *    rejected with S2DWC_ERROR_ARG_INVALID.
  *  - Setup: the first call on a device looks up the array's address
  *    (cudaGetSymbolAddress), which makes the CUDA driver load the module that
  *    holds it; make that first call during setup, before any stream capture.
+ *    The address is cached per device until s2dwc_finalize.  A
+ *    cudaDeviceReset unloads the module: call s2dwc_finalize after one, so
+ *    that the next call looks the address up again.
  *  - Nothing needs to start at zero: each call writes every scratch element
  *    before it reads it.
  *  - There is one scratch array per device: calls that overlap in time on one

@@ -35,6 +35,8 @@ SIGNATURES = {
     "s2dwc_synthesis_wav2flm_dynamic": (_i, [_dp, ctypes.POINTER(_dp), _dp, _dp, _dp, _dp, _i, _i, _i, _i, _d]),
     "s2dwc_plan_create": (_i, [ctypes.POINTER(_vp), _i, _i, _d, _i, _i, _i]),
     "s2dwc_plan_destroy": (_i, [_vp]),
+    "s2dwc_plan_footprint": (_i, [_i, _i, _d, _i, _i, _llp]),
+    "s2dwc_set_plan_memory_limit": (_i, [ctypes.c_longlong]),
     "s2dwc_plan_set_tables": (_i, [_vp, _dp, _dp, _dp, _i]),
     "s2dwc_plan_wav_offsets": (_i, [_vp, _llp]),
     "s2dwc_plan_workspace_bytes": (ctypes.c_longlong, [_vp]),

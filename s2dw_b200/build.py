@@ -43,15 +43,22 @@ def build(verbose=False, force=False):
     nvcc, cxx = _nvcc(), _host_cxx()
     common = ["-O3", "-std=c++17", "-lineinfo", "-ccbin", cxx,
               "-Xcompiler", "-fPIC,-fopenmp,-O3", "-I", os.path.join(HERE, "..", "include")]
-    objs = []
-    for s in srcs:
+    def compile_one(s):
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         cmd = [nvcc, "-c", s, "-o", o] + common + ARCH
         if s.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if verbose else []
+        return o, cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the translation units are independent: compile them concurrently
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, srcs))
+    objs = []
+    for s, (o, cmd, r) in zip(srcs, results):
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:
             sys.stdout.write(r.stdout)
             sys.stderr.write(r.stderr)

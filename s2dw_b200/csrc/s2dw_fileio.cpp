@@ -742,6 +742,7 @@ extern "C" {
 int s2dwc_fileio_fits_wav_write_dynamic(double *const *wav_scales, const double *scoeff, int J, int B, int N,
                                         int bl_scoeff, double alpha, const char *filename, const char *comment)
 {
+    S2DW_API_TRY
     int st = check_sizes("fits_wav_write_dynamic", J, B, N, bl_scoeff, alpha);
     if (st) return st;
     if (!wav_scales || !filename || (!scoeff && bl_scoeff > 0))
@@ -750,21 +751,25 @@ int s2dwc_fileio_fits_wav_write_dynamic(double *const *wav_scales, const double 
         if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "fits_wav_write_dynamic: scale %d is null", j);
     return fits_write(filename, scoeff, J, B, N, bl_scoeff, alpha, comment,
                       [&](int j) { return std::make_pair((const double *)wav_scales[j], 1LL); });
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_fits_wav_write_static(const double *wav, const double *scoeff, int J, int B, int N, int bl_scoeff,
                                        double alpha, const char *filename, const char *comment)
 {
+    S2DW_API_TRY
     int st = check_sizes("fits_wav_write_static", J, B, N, bl_scoeff, alpha);
     if (st) return st;
     if (!wav || !filename || (!scoeff && bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "fits_wav_write_static: null pointer");
     return fits_write(filename, scoeff, J, B, N, bl_scoeff, alpha, comment,
                       [&](int j) { return std::make_pair(wav + j, (long long)(J + 1)); });
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_fits_wav_read_header(const char *filename, int *J, int *B, int *N, int *bl_scoeff, double *alpha)
 {
+    S2DW_API_TRY
     File f;
     std::vector<Hdu> hdus;
     FitsHeader hd;
@@ -776,11 +781,13 @@ int s2dwc_fileio_fits_wav_read_header(const char *filename, int *J, int *B, int 
     if (bl_scoeff) *bl_scoeff = hd.bl_scoeff;
     if (alpha) *alpha = hd.alpha;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_fits_wav_read_dynamic(double *const *wav_scales, double *scoeff, int J, int B, int N, int bl_scoeff,
                                        const char *filename)
 {
+    S2DW_API_TRY
     File f;
     std::vector<Hdu> hdus;
     FitsHeader hd;
@@ -802,11 +809,13 @@ int s2dwc_fileio_fits_wav_read_dynamic(double *const *wav_scales, double *scoeff
                              filename);
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_fits_wav_read_static(double *wav, double *scoeff, int J, int B, int N, int bl_scoeff,
                                       const char *filename)
 {
+    S2DW_API_TRY
     File f;
     std::vector<Hdu> hdus;
     FitsHeader hd;
@@ -833,11 +842,13 @@ int s2dwc_fileio_fits_wav_read_static(double *wav, double *scoeff, int J, int B,
                     wav[j + (J + 1LL) * (a + (2LL * B - 1) * (b + 2LL * B * g))] = cube[(size_t)(a + na * (b + nb * g))];
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_matlab_wav_write_dynamic(double *const *wav_scales, const double *scoeff, int J, int B, int N,
                                           int bl_scoeff, double alpha, const char *filename, const char *comment)
 {
+    S2DW_API_TRY
     int st = check_sizes("matlab_wav_write_dynamic", J, B, N, bl_scoeff, alpha);
     if (st) return st;
     if (!wav_scales || !filename || (!scoeff && bl_scoeff > 0))
@@ -846,21 +857,25 @@ int s2dwc_fileio_matlab_wav_write_dynamic(double *const *wav_scales, const doubl
         if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "matlab_wav_write_dynamic: scale %d is null", j);
     return matlab_write(filename, scoeff, J, B, N, bl_scoeff, alpha, comment,
                         [&](int j) { return std::make_pair((const double *)wav_scales[j], 1LL); });
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_matlab_wav_write_static(const double *wav, const double *scoeff, int J, int B, int N, int bl_scoeff,
                                          double alpha, const char *filename, const char *comment)
 {
+    S2DW_API_TRY
     int st = check_sizes("matlab_wav_write_static", J, B, N, bl_scoeff, alpha);
     if (st) return st;
     if (!wav || !filename || (!scoeff && bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "matlab_wav_write_static: null pointer");
     return matlab_write(filename, scoeff, J, B, N, bl_scoeff, alpha, comment,
                         [&](int j) { return std::make_pair(wav + j, (long long)(J + 1)); });
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_matlab_wav_read_header(const char *filename, int *J, int *B, int *N, int *bl_scoeff, double *alpha)
 {
+    S2DW_API_TRY
     MatHeader hd;
     int st = matlab_header(filename, hd);
     if (st) return st;
@@ -870,11 +885,13 @@ int s2dwc_fileio_matlab_wav_read_header(const char *filename, int *J, int *B, in
     if (bl_scoeff) *bl_scoeff = hd.bl_scoeff;
     if (alpha) *alpha = hd.alpha;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_matlab_wav_read_dynamic(double *const *wav_scales, double *scoeff, int J, int B, int N,
                                          int bl_scoeff, const char *filename)
 {
+    S2DW_API_TRY
     MatHeader hd;
     int st = matlab_header(filename, hd);
     if (st) return st;
@@ -886,11 +903,13 @@ int s2dwc_fileio_matlab_wav_read_dynamic(double *const *wav_scales, double *scoe
     for (int j = 0; j <= J; j++)
         if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "matlab_wav_read_dynamic: scale %d is null", j);
     return matlab_read(filename, hd, scoeff, [&](int j) { return std::make_pair(wav_scales[j], 1LL); });
+    S2DW_API_CATCH
 }
 
 int s2dwc_fileio_matlab_wav_read_static(double *wav, double *scoeff, int J, int B, int N, int bl_scoeff,
                                         const char *filename)
 {
+    S2DW_API_TRY
     MatHeader hd;
     int st = matlab_header(filename, hd);
     if (st) return st;
@@ -901,6 +920,7 @@ int s2dwc_fileio_matlab_wav_read_static(double *wav, double *scoeff, int J, int 
         return set_error(S2DWC_ERROR_ARG_INVALID, "matlab_wav_read_static: null pointer");
     std::fill(wav, wav + (J + 1LL) * (2LL * B - 1) * 2LL * B * N, 0.0);
     return matlab_read(filename, hd, scoeff, [&](int j) { return std::make_pair(wav + j, (long long)(J + 1)); });
+    S2DW_API_CATCH
 }
 
 }  // extern "C"

@@ -140,10 +140,12 @@ extern "C" {
 
 int s2dwc_assimilate_int(double x, int *y)
 {
+    S2DW_API_TRY
     int t = 0;
     bool ok = assimilate_int(x, &t);
     if (y) *y = t;
     return ok ? 1 : 0;
+    S2DW_API_CATCH
 }
 
 int s2dwc_comp_jmax(int B, double alpha) { return comp_jmax(B, alpha); }
@@ -152,9 +154,11 @@ const char *s2dwc_last_error_message(void) { return g_last_msg; }
 
 int s2dwc_band_limits(int jj, int B, double alpha, int *bl_hi, int *bl_lo)
 {
+    S2DW_API_TRY
     if (!bl_hi || !bl_lo) return set_error(S2DWC_ERROR_ARG_INVALID, "band_limits: null output");
     band_limits(jj, B, alpha, bl_hi, bl_lo);
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 long long s2dwc_wav_scale_size(int jj, int B, int N, double alpha)
@@ -169,6 +173,7 @@ long long s2dwc_wav_scale_size(int jj, int B, int N, double alpha)
 // iteration, so the values match it.
 int s2dwc_init_kernels(double *K_gamma, double *Phi2, int *bl_scoeff, int J, int B, double alpha)
 {
+    S2DW_API_TRY
     if (!K_gamma || !Phi2 || !bl_scoeff)
         return set_error(S2DWC_ERROR_ARG_INVALID, "init_kernels: null pointer");
     if (B < 1 || !(alpha > 1.0) || !params_valid(J, B, alpha, -1))
@@ -217,6 +222,7 @@ int s2dwc_init_kernels(double *K_gamma, double *Phi2, int *bl_scoeff, int J, int
     if (status != S2DWC_OK)
         return set_error(status, "init_kernels: quadrature did not converge in 40 refinements");
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 // ln(n!) by the Lanczos series the reference uses (s2dw_core_mod.f90:1497-1544).
@@ -235,6 +241,7 @@ static double lanczos_logfact(int n)
 // s2dw_core_init_directionality, s2dw_core_mod.f90:219-250.
 int s2dwc_init_directionality(double *Slm_, int B, int N)
 {
+    S2DW_API_TRY
     if (!Slm_) return set_error(S2DWC_ERROR_ARG_INVALID, "init_directionality: null pointer");
     if (N > B || N < 1 || B < 1)
         return set_error(S2DWC_ERROR_SIZE_INVALID, "init_directionality: invalid N=%d B=%d", N, B);
@@ -254,11 +261,13 @@ int s2dwc_init_directionality(double *Slm_, int B, int N)
         }
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 // s2dw_core_admiss, s2dw_core_mod.f90:285-304.
 int s2dwc_admiss(double *admiss, const double *K_gamma, const double *Phi2, int B, int J, int *pass)
 {
+    S2DW_API_TRY
     if (!admiss || !K_gamma || !Phi2)
         return set_error(S2DWC_ERROR_ARG_INVALID, "admiss: null pointer");
     int ok = 1;
@@ -273,6 +282,7 @@ int s2dwc_admiss(double *admiss, const double *K_gamma, const double *Phi2, int 
     }
     if (pass) *pass = ok;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 }  // extern "C"

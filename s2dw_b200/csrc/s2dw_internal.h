@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -23,6 +25,25 @@ int set_error(int code, const char *fmt, ...);
             return ::s2dw::set_error(S2DWC_ERROR_CUDA, "%s failed: %s (%s:%d)", #call,   \
                                      cudaGetErrorString(e_), __FILE__, __LINE__);        \
     } while (0)
+
+// No C++ exception may cross the C ABI (a Fortran or ctypes caller would be
+// terminated): the body of every int-returning entry point runs inside
+// S2DW_API_TRY ... S2DW_API_CATCH, which turns a failed host allocation into
+// S2DWC_ERROR_MEM_ALLOC_FAIL and any other exception into
+// S2DWC_ERROR_ARG_INVALID with its message.
+#define S2DW_API_TRY try {
+#define S2DW_API_CATCH                                                                        \
+    }                                                                                         \
+    catch (const std::bad_alloc &) {                                                          \
+        return ::s2dw::set_error(S2DWC_ERROR_MEM_ALLOC_FAIL, "%s: host allocation failed",    \
+                                 __func__);                                                   \
+    }                                                                                         \
+    catch (const std::exception &ex_) {                                                       \
+        return ::s2dw::set_error(S2DWC_ERROR_ARG_INVALID, "%s: %s", __func__, ex_.what());    \
+    }                                                                                         \
+    catch (...) {                                                                             \
+        return ::s2dw::set_error(S2DWC_ERROR_ARG_INVALID, "%s: unexpected exception", __func__); \
+    }
 
 // ---------------------------------------------------------------------------
 // Host helpers restating the reference's scalar routines.
@@ -299,5 +320,7 @@ int launch_stat_moments(const StatArgs &a, cudaStream_t s);
 // Address on `device` (which must be current) of the static scratch array of
 // s2dwc_plan_analysis_noalloc, looked up once per device.
 int noalloc_scratch(int device, void **ptr);
+// Drops the cached addresses (s2dwc_finalize): the next call looks them up again.
+void noalloc_forget();
 
 }  // namespace s2dw

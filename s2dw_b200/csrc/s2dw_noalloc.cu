@@ -42,4 +42,10 @@ int noalloc_scratch(int device, void **ptr)
     return S2DWC_OK;
 }
 
+void noalloc_forget()
+{
+    std::lock_guard<std::mutex> g(g_mu);
+    for (auto &q : g_ptr) q = nullptr;
+}
+
 }  // namespace s2dw

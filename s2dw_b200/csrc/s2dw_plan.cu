@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <array>
 #include <cmath>
@@ -120,9 +121,13 @@ struct s2dwc_plan {
     int *st_flags = nullptr;
     std::vector<void *> allocs;
     std::mutex mu;  // serialises use of the workspaces
+    // footprint-only build (s2dwc_plan_footprint, the memory limit check of
+    // s2dwc_plan_create): allocations are counted, nothing touches a device
+    bool dry = false;
 
     ~s2dwc_plan()
     {
+        if (dry) return;
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(device);
@@ -148,11 +153,25 @@ struct s2dwc_plan {
 
 namespace {
 
+// Process-wide limit on the device bytes one plan may hold (0: none), set by
+// s2dwc_set_plan_memory_limit.
+std::atomic<long long> g_plan_mem_limit{0};
+
 template <typename T>
 int dev_alloc(s2dwc_plan *p, T **ptr, size_t count)
 {
     void *v = nullptr;
     if (count == 0) count = 1;
+    if (p->dry) {
+        p->ws_bytes += (long long)(count * sizeof(T));
+        *ptr = nullptr;
+        return S2DWC_OK;
+    }
+    const long long lim = g_plan_mem_limit.load();
+    if (lim > 0 && p->ws_bytes + (long long)(count * sizeof(T)) > lim)
+        return set_error(S2DWC_ERROR_MEM_ALLOC_FAIL,
+                         "plan memory limit: %zu more bytes would take the plan to %lld bytes, above the "
+                         "limit of %lld", count * sizeof(T), p->ws_bytes + (long long)(count * sizeof(T)), lim);
     cudaError_t e = cudaMalloc(&v, count * sizeof(T));
     if (e != cudaSuccess)
         return set_error(S2DWC_ERROR_MEM_ALLOC_FAIL, "cudaMalloc of %zu bytes failed: %s",
@@ -183,7 +202,20 @@ int dev_upload(s2dwc_plan *p, T **ptr, const std::vector<T> &h)
 {
     int st = dev_alloc(p, ptr, h.size());
     if (st) return st;
+    if (p->dry) return S2DWC_OK;
     S2DW_CUDA_TRY(cudaMemcpy(*ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return S2DWC_OK;
+}
+
+// Twiddle tables of FFT length M, built with the plan: a status instead of an
+// exception (std::map::at) or a default entry (operator[]) if one is missing.
+int plan_tw(const s2dwc_plan *p, int M, TwDev *out)
+{
+    auto it = p->tw.find(M);
+    if (it == p->tw.end())
+        return set_error(S2DWC_ERROR_ARG_INVALID, "no twiddle table of length %d in the plan (B=%d N=%d)", M, p->B,
+                         p->N);
+    *out = it->second;
     return S2DWC_OK;
 }
 
@@ -363,6 +395,7 @@ int plan_build(s2dwc_plan *p)
         p->mw_tiles.push_back(d);
         p->mw_ntiles.push_back(p->bl[j] - p->blo[j] - 1 > 0 ? (int)tl.size() : 0);
     }
+    if (p->dry) return S2DWC_OK;
     p->streams.resize(J + 1);
     p->ev_join.resize(J + 1);
     for (int j = 0; j <= J; j++) {
@@ -513,7 +546,7 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
         ca.rows = p->N * bl;
         ca.czt = p->czt[j][ca.mode];
-        ca.tw = p->tw[ca.czt.M];
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_c = Tg;
         ca.out_c = Tb;
         {
@@ -523,7 +556,7 @@ int run_analysis(s2dwc_plan *p, double *d_wav, double2 *d_scoeff, const double2 
         ca.mode = CZT_ANA_ALPHA;
         ca.rows = p->N * bl;  // (g, b pair)
         ca.czt = p->czt[j][CZT_ANA_ALPHA];
-        ca.tw = p->tw[ca.czt.M];
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_c = Tb;
         ca.out_c = nullptr;
         ca.out_r = d_wav + p->wav_off[j];
@@ -569,7 +602,7 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
         ca.rows = p->N * bl;
         ca.czt = p->czt[j][CZT_SYN_ALPHA];
-        ca.tw = p->tw[ca.czt.M];
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_r = d_wav + p->wav_off[j];
         ca.out_c = Vw;
         ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
@@ -580,7 +613,7 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ca.mode = p->syn_beta_mode[j];
         ca.rows = p->NP * bl;
         ca.czt = p->czt[j][ca.mode];
-        ca.tw = p->tw[ca.czt.M];
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_c = Vw;
         ca.in_r = nullptr;
         ca.out_c = V2f;
@@ -703,14 +736,14 @@ int run_analysis_serial(const s2dwc_plan *p, unsigned char *ws, double *d_wav, d
         std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
         ca.rows = p->N * bl;
         ca.czt = p->czt[j][ca.mode];
-        ca.tw = p->tw.at(ca.czt.M);
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_c = Tg;
         ca.out_c = Tb;
         if ((st = launch_czt(ca, s))) return st;
         ca.mode = CZT_ANA_ALPHA;
         ca.rows = p->N * bl;
         ca.czt = p->czt[j][CZT_ANA_ALPHA];
-        ca.tw = p->tw.at(ca.czt.M);
+        if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
         ca.in_c = Tb;
         ca.out_c = nullptr;
         ca.out_r = d_wav + p->wav_off[j];
@@ -954,7 +987,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
                 std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
                 ca.rows = p->N * bl;
                 ca.czt = p->czt[j][ca.mode];
-                ca.tw = p->tw.at(ca.czt.M);
+                if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
                 ca.in_c = p->sp_Tg + p->sp_cap * S.tg_off + (long long)k * p->N * bl * bl;
                 ca.out_c = p->sp_Tb + S.tb_off;
                 {
@@ -963,7 +996,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
                 }
                 ca.mode = CZT_ANA_ALPHA;
                 ca.czt = p->czt[j][CZT_ANA_ALPHA];
-                ca.tw = p->tw.at(ca.czt.M);
+                if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
                 ca.in_c = p->sp_Tb + S.tb_off;
                 ca.out_c = nullptr;
                 ca.out_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
@@ -1013,7 +1046,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
                 std::memcpy(ca.nq, p->nq, sizeof(ca.nq));
                 ca.rows = p->N * bl;
                 ca.czt = p->czt[j][CZT_SYN_ALPHA];
-                ca.tw = p->tw.at(ca.czt.M);
+                if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
                 ca.in_r = d_wav + (g0 + k) * wtot + p->wav_off[j];
                 ca.out_c = p->sp_Tb + S.tb_off;
                 ca.scale = (4.0 * (M_PI * M_PI) / (double)p->N) / (2.0 * bl - 1.0);
@@ -1024,7 +1057,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
                 ca.mode = p->syn_beta_mode[j];
                 ca.rows = p->NP * bl;
                 ca.czt = p->czt[j][ca.mode];
-                ca.tw = p->tw.at(ca.czt.M);
+                if ((st = plan_tw(p, ca.czt.M, &ca.tw))) return st;
                 ca.in_c = p->sp_Tb + S.tb_off;
                 ca.in_r = nullptr;
                 ca.out_c = p->sp_V2f + p->sp_cap * S.v2f_off + k * S.vstride;
@@ -1105,15 +1138,20 @@ const char *s2dwc_version(void) { return "s2dw-b200 0.1 (sm_100a, FP64)"; }
 
 int s2dwc_init(void)
 {
+    S2DW_API_TRY
     S2DW_CUDA_TRY(cudaFree(nullptr));
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_finalize(void)
 {
+    S2DW_API_TRY
     std::lock_guard<std::mutex> g(g_cache_mu);
     g_cache.clear();
+    noalloc_forget();
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 const char *s2dwc_error_string(int code)
@@ -1142,6 +1180,7 @@ const char *s2dwc_error_string(int code)
 
 int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int form, int device)
 {
+    S2DW_API_TRY
     if (!plan) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_create: null output");
     *plan = nullptr;
     int st = validate_sizes(B, N, alpha, J);
@@ -1150,6 +1189,15 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
     if (form == S2DWC_FORM_SPLIT && N > 8)
         return set_error(S2DWC_ERROR_SIZE_INVALID, "N=%d: the split form supports N <= 8", N);
+    if (const long long lim = g_plan_mem_limit.load()) {
+        // checked on the host before any device call
+        long long need = 0;
+        if ((st = s2dwc_plan_footprint(B, N, alpha, J, form, &need))) return st;
+        if (need > lim)
+            return set_error(S2DWC_ERROR_MEM_ALLOC_FAIL,
+                             "plan B=%d N=%d J=%d needs %lld bytes of device memory, above the plan memory "
+                             "limit of %lld", B, N, J, need, lim);
+    }
     int ndev = 0;
     S2DW_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev)
@@ -1178,17 +1226,50 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     }
     *plan = p;
     return S2DWC_OK;
+    S2DW_API_CATCH
+}
+
+int s2dwc_plan_footprint(int B, int N, double alpha, int J, int form, long long *bytes)
+{
+    S2DW_API_TRY
+    if (!bytes) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_footprint: null output");
+    *bytes = 0;
+    int st = validate_sizes(B, N, alpha, J);
+    if (st) return st;
+    if (form != S2DWC_FORM_FP64 && form != S2DWC_FORM_SPLIT)
+        return set_error(S2DWC_ERROR_ARG_INVALID, "unknown form %d", form);
+    s2dwc_plan p;
+    p.dry = true;
+    p.B = B;
+    p.N = N;
+    p.J = J;
+    p.alpha = alpha;
+    p.form = form;
+    if ((st = plan_build(&p))) return st;
+    *bytes = p.ws_bytes;
+    return S2DWC_OK;
+    S2DW_API_CATCH
+}
+
+int s2dwc_set_plan_memory_limit(long long bytes)
+{
+    if (bytes < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan memory limit %lld is negative", bytes);
+    g_plan_mem_limit.store(bytes);
+    return S2DWC_OK;
 }
 
 int s2dwc_plan_destroy(s2dwc_plan *plan)
 {
+    S2DW_API_TRY
     delete plan;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Phi2, const double *Slm_,
                           int bl_scoeff)
 {
+    S2DW_API_TRY
     if (!p || !K_gamma || !Slm_) return set_error(S2DWC_ERROR_ARG_INVALID, "set_tables: null pointer");
     const int B = p->B, N = p->N, J = p->J, NP = p->NP;
     if (bl_scoeff < 0 || bl_scoeff > B)
@@ -1292,19 +1373,23 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
     p->tables_set = true;
     p->sp_dexp_valid = false;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_wav_offsets(const s2dwc_plan *p, long long *offsets)
 {
+    S2DW_API_TRY
     if (!p || !offsets) return set_error(S2DWC_ERROR_ARG_INVALID, "wav_offsets: null pointer");
     for (int j = 0; j <= p->J + 1; j++) offsets[j] = p->wav_off[j];
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 long long s2dwc_plan_workspace_bytes(const s2dwc_plan *p) { return p ? p->ws_bytes : 0; }
 
 int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
 {
+    S2DW_API_TRY
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "launch_count: null plan");
     // a general Slm runs each contraction twice
     const int g = p->slm_general ? 2 : 1;
@@ -1313,17 +1398,21 @@ int s2dwc_plan_launch_count(const s2dwc_plan *p, int *analysis, int *synthesis)
     for (int j = 0; j <= p->J; j++) ns += 2 + ((p->bl[j] - p->blo[j] - 1) > 0 ? g : 0);
     if (synthesis) *synthesis = ns;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_set_timing(s2dwc_plan *p, int enable)
 {
+    S2DW_API_TRY
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "set_timing: null plan");
     p->timing = enable != 0;
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_timing(s2dwc_plan *p, int kind, long long *launches, double *total_ms)
 {
+    S2DW_API_TRY
     if (!p || kind < 0 || kind >= S2DWC_KIND_COUNT)
         return set_error(S2DWC_ERROR_ARG_INVALID, "timing: bad plan or kind %d", kind);
     DeviceGuard dg(p->device);
@@ -1340,10 +1429,12 @@ int s2dwc_plan_timing(s2dwc_plan *p, int kind, long long *launches, double *tota
     if (launches) *launches = p->t_n[kind];
     if (total_ms) *total_ms = p->t_ms[kind];
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_timing_reset(s2dwc_plan *p)
 {
+    S2DW_API_TRY
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "timing_reset: null plan");
     long long n;
     double ms;
@@ -1353,10 +1444,12 @@ int s2dwc_plan_timing_reset(s2dwc_plan *p)
         p->t_n[k] = 0;
     }
     return st;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_analysis(s2dwc_plan *p, double *d_wav, double *d_scoeff, const double *d_flm, void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis: null pointer");
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis: tables not set");
@@ -1366,11 +1459,13 @@ int s2dwc_plan_analysis(s2dwc_plan *p, double *d_wav, double *d_scoeff, const do
                                   reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
     return run_analysis(p, d_wav, reinterpret_cast<double2 *>(d_scoeff),
                         reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_analysis_batch(s2dwc_plan *p, int nmaps, double *d_wav, double *d_scoeff, const double *d_flm,
                               void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_batch: null pointer");
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_batch: nmaps=%d", nmaps);
@@ -1388,11 +1483,13 @@ int s2dwc_plan_analysis_batch(s2dwc_plan *p, int nmaps, double *d_wav, double *d
         if (st) return st;
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const double *d_wav, const double *d_scoeff,
                                void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: null pointer");
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: nmaps=%d", nmaps);
@@ -1410,11 +1507,13 @@ int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const do
         if (st) return st;
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_stat_moments(s2dwc_plan *p, int nmaps, const double *d_wav, const double *d_mask, double *d_moments,
                             void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_moments) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_stat_moments: null pointer");
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_stat_moments: nmaps=%d", nmaps);
     DeviceGuard dg(p->device);
@@ -1442,11 +1541,13 @@ int s2dwc_plan_stat_moments(s2dwc_plan *p, int nmaps, const double *d_wav, const
         if ((st = launch_stat_moments(a, (cudaStream_t)stream))) return st;
     }
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double alpha, double *mean, double *var,
                        double *skew, double *kur, const double *const *mask_scales, double *five, double *six)
 {
+    S2DW_API_TRY
     if (!wav_scales || !mean || !var || !skew || !kur)
         return set_error(S2DWC_ERROR_ARG_INVALID, "stat_moments: null pointer");
     if (B < 2 || N < 1 || J < 0 || J > S2DW_JMAX || !(alpha > 1.0))
@@ -1518,10 +1619,12 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
                                "stat_moments: scale %d has zero variance; its higher moments are set to zero", j);
     }
     return status;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_reserve(s2dwc_plan *p, int nmaps, void *stream)
 {
+    S2DW_API_TRY
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_reserve: null plan");
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_reserve: nmaps=%d", nmaps);
     if (p->form != S2DWC_FORM_SPLIT) return S2DWC_OK;
@@ -1529,10 +1632,12 @@ int s2dwc_plan_reserve(s2dwc_plan *p, int nmaps, void *stream)
     DeviceGuard dg(p->device);
     std::lock_guard<std::mutex> g(p->mu);
     return split_prepare(p, nmaps, (cudaStream_t)stream);
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_check(s2dwc_plan *p)
 {
+    S2DW_API_TRY
     if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_check: null plan");
     if (!p->sp_err) return S2DWC_OK;
     DeviceGuard dg(p->device);
@@ -1540,10 +1645,12 @@ int s2dwc_plan_check(s2dwc_plan *p)
     S2DW_CUDA_TRY(cudaMemcpy(&h, p->sp_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) return set_error(S2DWC_ERROR_CUDA, "a split-form kernel gave up waiting for its tensor-core pipeline");
     return S2DWC_OK;
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, const double *d_scoeff, void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis: null pointer");
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis: tables not set");
@@ -1553,19 +1660,24 @@ int s2dwc_plan_synthesis(s2dwc_plan *p, double *d_flm, const double *d_wav, cons
                                    reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
     return run_synthesis(p, reinterpret_cast<double2 *>(d_flm), d_wav,
                          reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
+    S2DW_API_CATCH
 }
 
 int s2dwc_plan_analysis_noalloc(const s2dwc_plan *p, double *d_wav, double *d_scoeff, const double *d_flm,
                                 void *stream)
 {
+    S2DW_API_TRY
     if (!p || !d_wav || !d_flm || (!d_scoeff && p->bl_scoeff > 0))
         return set_error(S2DWC_ERROR_ARG_INVALID, "plan_analysis_noalloc: null pointer");
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis_noalloc: tables not set");
+    if (p->form != S2DWC_FORM_FP64)
+        return set_error(S2DWC_ERROR_ARG_INVALID,
+                         "plan_analysis_noalloc runs the FP64 form only; create the plan with S2DWC_FORM_FP64");
     const SerialLayout L = serial_layout(p);
     if (L.bytes > S2DWC_NOALLOC_SCRATCH_BYTES)
         return set_error(S2DWC_ERROR_SIZE_INVALID,
                          "plan_analysis_noalloc: B=%d N=%d needs %lld bytes of scratch, more than the "
-                         "%lld-byte static scratch (it holds B<=256 at any N<=8, or B=512 at N<=2); "
+                         "%lld-byte static scratch (it holds B<=256 with N<=10, or B<=512 with N<=2); "
                          "use s2dwc_plan_analysis",
                          p->B, p->N, L.bytes, (long long)S2DWC_NOALLOC_SCRATCH_BYTES);
     DeviceGuard dg(p->device);
@@ -1574,6 +1686,7 @@ int s2dwc_plan_analysis_noalloc(const s2dwc_plan *p, double *d_wav, double *d_sc
     if (st) return st;
     return run_analysis_serial(p, static_cast<unsigned char *>(ws), d_wav, reinterpret_cast<double2 *>(d_scoeff),
                                reinterpret_cast<const double2 *>(d_flm), (cudaStream_t)stream);
+    S2DW_API_CATCH
 }
 
 // ---------------------------------------------------------------------------
@@ -1862,18 +1975,22 @@ static int analysis_host(double *wav_static, double *const *wav_scales, double *
 int s2dwc_analysis_flm2wav(double *wav, double *scoeff, const double *flm, const double *K_gamma,
                            const double *Slm, int J, int B, int N, int bl_scoeff, double alpha)
 {
+    S2DW_API_TRY
     if (!wav) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null wav");
     return analysis_host(wav, nullptr, scoeff, flm, K_gamma, Slm, J, B, N, bl_scoeff, alpha);
+    S2DW_API_CATCH
 }
 
 int s2dwc_analysis_flm2wav_dynamic(double *const *wav_scales, double *scoeff, const double *flm,
                                    const double *K_gamma, const double *Slm, int J, int B, int N,
                                    int bl_scoeff, double alpha)
 {
+    S2DW_API_TRY
     if (!wav_scales) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: null wav_scales");
     for (int j = 0; j <= J; j++)
         if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "analysis: wav_scales[%d] is null", j);
     return analysis_host(nullptr, wav_scales, scoeff, flm, K_gamma, Slm, J, B, N, bl_scoeff, alpha);
+    S2DW_API_CATCH
 }
 
 static int synthesis_host(double *flm, const double *wav_static, const double *const *wav_scales,
@@ -1948,18 +2065,22 @@ int s2dwc_synthesis_wav2flm(double *flm, const double *wav, const double *scoeff
                             const double *Phi2, const double *Slm, int J, int B, int N, int bl_scoeff,
                             double alpha)
 {
+    S2DW_API_TRY
     if (!wav) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null wav");
     return synthesis_host(flm, wav, nullptr, scoeff, K_gamma, Phi2, Slm, J, B, N, bl_scoeff, alpha);
+    S2DW_API_CATCH
 }
 
 int s2dwc_synthesis_wav2flm_dynamic(double *flm, const double *const *wav_scales, const double *scoeff,
                                     const double *K_gamma, const double *Phi2, const double *Slm, int J,
                                     int B, int N, int bl_scoeff, double alpha)
 {
+    S2DW_API_TRY
     if (!wav_scales) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: null wav_scales");
     for (int j = 0; j <= J; j++)
         if (!wav_scales[j]) return set_error(S2DWC_ERROR_ARG_INVALID, "synthesis: wav_scales[%d] is null", j);
     return synthesis_host(flm, nullptr, wav_scales, scoeff, K_gamma, Phi2, Slm, J, B, N, bl_scoeff, alpha);
+    S2DW_API_CATCH
 }
 
 }  // extern "C"

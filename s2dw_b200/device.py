@@ -15,6 +15,20 @@ from ._lib import check, lib
 from .core import band_limits
 
 
+def plan_footprint(B, N, alpha, J, form=0):
+    """Device bytes a plan for (B, N, alpha, J, form) allocates when created,
+    computed on the host (no device is touched)."""
+    out = ctypes.c_longlong(0)
+    check(lib().s2dwc_plan_footprint(int(B), int(N), float(alpha), int(J), int(form), ctypes.byref(out)))
+    return int(out.value)
+
+
+def set_plan_memory_limit(nbytes):
+    """Process-wide limit on one plan's device memory (0: none).  Plans above
+    it are refused with S2DW_ERROR_MEM_ALLOC_FAIL (4) before any device call."""
+    check(lib().s2dwc_set_plan_memory_limit(int(nbytes)))
+
+
 class Plan:
     FP64, SPLIT = 0, 1
 

@@ -65,3 +65,72 @@ def test_noalloc_rejects_plans_beyond_the_scratch():
         plan.analysis_noalloc(d_flm, d_wav, d_sc)
     assert ei.value.code == 8 and "static scratch" in str(ei.value)
     plan.close()
+
+
+def _general_slm(B, N, seed):
+    """A complex Slm not of the init_directionality form, on the n the
+    transform uses: the analysis then runs its second contraction (the
+    imaginary part of S/eta) through the same scratch."""
+    rng = np.random.default_rng(seed)
+    S = np.zeros((B, N), dtype=np.complex128, order="F")
+    for n in range(N):
+        if (N + n) % 2 == 1:
+            S[n:, n] = rng.standard_normal(B - n) + 1j * rng.standard_normal(B - n)
+    return S
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha", [(64, 4, 2.0), (256, 10, 2.0)])
+def test_noalloc_general_slm_and_largest_n(B, N, alpha):
+    """A random complex Slm at B=64 and the largest N the scratch holds at
+    B=256 (N=10: 31 MiB of the 32 MiB), two calls in a row each."""
+    import torch
+
+    from s2dw_b200.device import Plan
+
+    t = transform_setup(B, N, alpha)
+    S = _general_slm(B, N, seed=B + N) if B == 64 else t["Slm"]
+    plan = Plan(B, N, alpha, t["J"])
+    plan.set_tables(t["K_gamma"], t["Phi2"], S, t["bl_scoeff"])
+    for call, seed in enumerate((21, 22)):
+        d_flm, d_ref, d_sc_ref = _device_inputs(plan, t, B, seed)
+        d_wav = torch.full_like(d_ref, np.nan)
+        d_sc = torch.full_like(d_sc_ref, np.nan)
+        plan.analysis(d_flm, d_ref, d_sc_ref)
+        plan.analysis_noalloc(d_flm, d_wav, d_sc)
+        torch.cuda.synchronize()
+        ref, got = d_ref.cpu().numpy(), d_wav.cpu().numpy()
+        assert np.isfinite(got).all(), f"call {call}: non-finite output"
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err <= TOL, f"call {call}: max|dw|/max|w| = {err:.3e}"
+        np.testing.assert_array_equal(d_sc.cpu().numpy(), d_sc_ref.cpu().numpy())
+    plan.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_split_form_and_n_beyond_the_scratch():
+    """The entry point runs the FP64 form only: a split-form plan gets
+    S2DW_ERROR_ARG_INVALID (10).  B=256 with N=11 needs 34.6 MB of scratch and
+    gets S2DW_ERROR_SIZE_INVALID (8)."""
+    from s2dw_b200._lib import S2DWError
+    from s2dw_b200.device import Plan
+
+    B, N, alpha = 64, 4, 2.0
+    t = transform_setup(B, N, alpha)
+    sp = Plan(B, N, alpha, t["J"], form=Plan.SPLIT)
+    sp.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    d_flm, d_wav, d_sc = _device_inputs(sp, t, B, 0)
+    with pytest.raises(S2DWError) as ei:
+        sp.analysis_noalloc(d_flm, d_wav, d_sc)
+    assert ei.value.code == 10 and "FP64 form" in str(ei.value)
+    sp.close()
+
+    B, N = 256, 11
+    t = transform_setup(B, N, alpha)
+    plan = Plan(B, N, alpha, t["J"])
+    plan.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    d_flm, d_wav, d_sc = _device_inputs(plan, t, B, 0)
+    with pytest.raises(S2DWError) as ei:
+        plan.analysis_noalloc(d_flm, d_wav, d_sc)
+    assert ei.value.code == 8
+    plan.close()
