@@ -57,7 +57,8 @@ NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.60e6, "mwalk": 10.76e6, "ana_beta": 2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 300; 10 for --impl reference, whose steps are CPU pairs)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--B", type=int, default=1024)
@@ -419,68 +420,109 @@ def measured_fp64_peak():
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_baseline(B, N, alpha, budget_s=30.0):
-    """CPU restatement of the reference timed on the host cores on a bounded
-    sample: each O(bl^3) loop runs every s-th iteration; two strides s and
-    2s give t(s) = c + h/s, so the full pair costs c + h."""
-    from oracle import oracle as O
+def _generator():
+    """The seeded flm generator (s2dw_b200/workload.py, numpy only), loaded by
+    file path so that the CPU legs do not import the s2dw_b200 package."""
+    import importlib.util
 
-    from s2dw_b200.workload import gaussian_flm, transform_setup
+    spec = importlib.util.spec_from_file_location("s2dw_workload_gen", os.path.join(ROOT, "s2dw_b200", "workload.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.gaussian_flm
 
-    threads = min(os.cpu_count() or 1, 64)
-    O.set_num_threads(threads)
-    t = transform_setup(B, N, alpha)
-    flm = gaussian_flm(B, seed=0)
-    a = (t["K_gamma"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
-    s_ = (t["K_gamma"], t["Phi2"], t["Slm"], t["J"], B, N, t["bl_scoeff"], alpha)
 
-    def run(stride):
-        O.set_sample_stride(stride)
+def _cpu_threads():
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, min(n, 64))
+
+
+class CpuPair:
+    """The CPU restatement of the reference (oracle/, C + OpenMP, the
+    reference's loops including its naive beta sums) on one configuration:
+    tables from the oracle's own init_kernels / init_directionality, the
+    seeded flm of the benchmark.  Nothing of the CUDA library is loaded."""
+
+    def __init__(self, B, N, alpha, seed=0, threads=None):
+        from oracle import oracle as O
+
+        self.O = O
+        self.threads = threads or _cpu_threads()
+        O.set_num_threads(self.threads)
+        J = O.comp_jmax(B, alpha)
+        K, P, bs = O.init_kernels(J, B, alpha)
+        S = O.init_directionality(B, N)
+        self.flm = _generator()(B, seed=seed)
+        self.a = (K, S, J, B, N, bs, alpha)
+        self.s = (K, P, S, J, B, N, bs, alpha)
+        self.B, self.N, self.J = B, N, J
+
+    def pair(self):
+        """One full analysis + synthesis; returns (seconds, recon error)."""
         t0 = time.perf_counter()
-        w, sc = O.analysis_dynamic(flm, *a)
-        O.synthesis_dynamic(w, sc, *s_)
-        return time.perf_counter() - t0
+        w, sc = self.O.analysis_dynamic(self.flm, *self.a)
+        f = self.O.synthesis_dynamic(w, sc, *self.s)
+        dt = time.perf_counter() - t0
+        return dt, float(np.abs(f - self.flm).max())
 
-    s1 = 32 if B >= 1024 else 8
-    t1 = run(s1)
-    t2 = run(s1 // 2)
-    O.set_sample_stride(1)
-    h = max((t2 - t1) / (1.0 / (s1 // 2) - 1.0 / s1), 0.0)
-    c = max(t1 - h / s1, 0.0)
-    full = c + h
-    return {"value": 1.0 / full, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"CPU restatement (C/OpenMP) of the reference loops at B={B} N={N}: every {s1}-th and "
-                       f"{s1 // 2}-th iteration of each O(bl^3) loop, fitted t(s)=c+h/s -> {full:.1f} s/pair "
-                       f"(sampled runs {t1:.1f}s, {t2:.1f}s)")}
+
+def cpu_baseline(B, N, alpha):
+    """The CPU restatement timed on the host cores: one full, unsampled
+    analysis+synthesis pair of the benchmark configuration (every scale,
+    every loop iteration), after one untimed warm-up pair at B=128."""
+    CpuPair(128, N, alpha).pair()
+    cp = CpuPair(B, N, alpha)
+    dt, err = cp.pair()
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": cp.threads, "kind": "port",
+            "sample": (f"one full unsampled analysis+synthesis pair at B={B} N={N} alpha={alpha:g} J={cp.J} "
+                       f"(all scales; CPU restatement of the reference loops in C/OpenMP, {cp.threads} threads): "
+                       f"{dt:.1f} s, reconstruction error {err:.1e}"),
+            "recon_err": err}
 
 
 def run_reference(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    """The reference arm: the CPU restatement of the reference (oracle/,
+    the reference's Fortran/FFTW cannot be compiled here) on the host cores.
+    Warm-up steps are pairs at B=128 (threads and pages warm); each timed
+    step is one full unsampled analysis+synthesis pair of the benchmark
+    configuration.  Only the oracle's library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     B, N, alpha = args.B, args.N, args.alpha
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(B, N, alpha)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+    warm = CpuPair(128, N, alpha)
+    for _ in range(args.warmup):
+        warm.pair()
+    cp = CpuPair(B, N, alpha)
+    times, errs = [], []
+    for _ in range(args.steps):
+        dt, err = cp.pair()
+        times.append(dt)
+        errs.append(err)
+    total = sum(times)
+    v = args.steps / total
+    cb = {"value": v, "unit": UNIT, "cores": cp.threads, "kind": "port",
+          "sample": (f"{args.steps} full unsampled analysis+synthesis pairs at B={B} N={N} alpha={alpha:g} "
+                     f"J={cp.J} (all scales; CPU restatement of the reference loops in C/OpenMP, {cp.threads} "
+                     f"threads), {total:.1f} s in all, {min(times):.1f}-{max(times):.1f} s per pair; "
+                     f"warm-up: {args.warmup} pairs at B=128")}
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian C_l=1/(l(l+1)) flm)",
-            "impl": "reference",
-            "config": {"workload": f"B={B} N={N} alpha={alpha:g} J=Jmax analysis+synthesis of one map",
-                       "B": B, "N": N, "alpha": alpha},
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian C_l=1/(l(l+1)) flm)", "impl": "reference",
+            "config": {"workload": f"B={B} N={N} alpha={alpha:g} J=Jmax={cp.J} analysis+synthesis of one map",
+                       "B": B, "N": N, "alpha": alpha, "J": cp.J, "recon_err": max(errs)},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    del world
 
 
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = 10 if args.impl == "reference" else 300
     if args.impl == "reference":
         run_reference(args)
         return

@@ -64,7 +64,6 @@ def lib():
                                            ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.orc_ran2_reset.argtypes = []
         L.orc_test_gen_flm.argtypes = [ctypes.c_int, _dp, ctypes.c_int32]
-        L.orc_set_sample_stride.argtypes = [ctypes.c_int]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -81,12 +80,6 @@ def _p(a):
 def _check(status, what):
     if status != 0:
         raise RuntimeError(f"oracle {what} failed with S2DW error code {status}")
-
-
-def set_sample_stride(s):
-    """CPU-baseline timing only: process every s-th iteration of each
-    O(bl^3) loop (results are then meaningless)."""
-    lib().orc_set_sample_stride(int(s))
 
 
 def num_threads():

@@ -47,15 +47,6 @@ typedef double complex dcx;
 #define ORC_TOL_LIMIT 1e-12
 #define ORC_TOL_CEIL 1e-5
 
-/* Work sampling for the timed CPU baseline only: when orc_stride > 1, each
- * O(bl^3) loop nest (contraction over el, beta sums over b or m', the alpha
- * FFT loops, the Wigner sum over el) processes only every orc_stride-th
- * iteration, so that the elapsed time times orc_stride estimates the full
- * transform.  Results are meaningless in that mode. */
-static int orc_stride = 1;
-void orc_set_sample_stride(int s) { orc_stride = s > 1 ? s : 1; }
-#define ORC_SKIP(i) (orc_stride > 1 && ((i) % orc_stride) != 0)
-
 /* error codes, s2dw_error_mod.f90:37-52 */
 enum { ORC_OK = 0, ORC_ERR_MEM = 4, ORC_ERR_ARTH = 5, ORC_ERR_SIZE = 8,
        ORC_ERR_QUAD = 12, ORC_ERR_ADMISS = 13 };
@@ -467,7 +458,6 @@ int orc_analysis_scale(int jj, double *out, size_t astride, size_t bstride, size
         double *dl = (double *)malloc(sizeof(double) * (size_t)(2 * bl + 1) * (2 * bl + 1));
 #pragma omp for schedule(dynamic, 10)
         for (int el = bl_lo + 1; el <= bl_hi - 1; el++) {
-            if (ORC_SKIP(el - bl_lo - 1)) continue;
             orc_dl_beta_operator(dl, ORC_PION2, el);
             const size_t w = (size_t)(2 * el + 1);
 #define D(i, k) dl[((i) + el) + w * ((k) + el)]
@@ -523,7 +513,6 @@ int orc_analysis_scale(int jj, double *out, size_t astride, size_t bstride, size
 #pragma omp parallel for collapse(2) schedule(dynamic, 10)
     for (int gg = 0; gg <= N - 1; gg++) {
         for (int bb = 0; bb <= 2 * bl - 1; bb++) {
-            if (ORC_SKIP(bb)) continue;
             double beta_b = ORC_PI * (2.0 * bb + 1.0) / (4.0 * bl);
             for (int mm = 0; mm <= bl - 1; mm++) {
                 double cb = 2.0 * cos(mm * beta_b), sbv = 2.0 * sin(mm * beta_b);
@@ -551,7 +540,6 @@ int orc_analysis_scale(int jj, double *out, size_t astride, size_t bstride, size
 #pragma omp for collapse(2) schedule(dynamic, 10)
         for (int gg = 0; gg <= N - 1; gg++) {
             for (int bb = 0; bb <= 2 * bl - 1; bb++) {
-                if (ORC_SKIP(bb)) continue;
                 const dcx *X = Tmbg + (size_t)bl * bb + nB * gg;
                 x[0] = creal(X[0]);
                 for (int m = 1; m < bl; m++) { x[m] = X[m]; x[n - m] = conj(X[m]); }
@@ -627,7 +615,6 @@ int orc_synthesis_scale(int jj, dcx *flm, const double *in, size_t astride, size
 #pragma omp for collapse(2) schedule(dynamic, 10)
         for (int gg = 0; gg <= N - 1; gg++) {
             for (int bb = 0; bb <= 2 * bl - 1; bb++) {
-                if (ORC_SKIP(bb)) continue;
                 for (int a = 0; a < n; a++) x[a] = in[astride * a + bstride * bb + gstride * gg];
                 orc_fft_exec(&P, x, y, scr);
                 for (int m = 0; m < bl; m++) VV(m, bb, gg) = y[m] * c1 / c2;
@@ -666,7 +653,6 @@ int orc_synthesis_scale(int jj, dcx *flm, const double *in, size_t astride, size
     for (int mmm = 0; mmm <= N - 1; mmm++) {
         for (int mm = -(bl - 1); mm <= bl - 1; mm++) {
             if ((N + mmm) % 2 == 0) continue;
-            if (ORC_SKIP(mm + bl - 1)) continue;
             for (int bb = 0; bb <= 2 * bl - 1; bb++) {
                 double beta_b = ORC_PI * (2.0 * bb + 1.0) / (4.0 * bl);
                 dcx e = cexp(-(I * (mm * beta_b)));
@@ -694,7 +680,6 @@ int orc_synthesis_scale(int jj, dcx *flm, const double *in, size_t astride, size
         double *dl = (double *)malloc(sizeof(double) * (size_t)(2 * bl + 1) * (2 * bl + 1));
 #pragma omp for schedule(dynamic, 10)
         for (int el = bl_lo + 1; el <= bl_hi - 1; el++) {
-            if (ORC_SKIP(el - bl_lo - 1)) continue;
             orc_dl_beta_operator(dl, ORC_PION2, el);
             const size_t w = (size_t)(2 * el + 1);
 #define D(i, k) dl[((i) + el) + w * ((k) + el)]

@@ -32,3 +32,25 @@ def test_contraction_flops_split_by_kind():
     ana, syn = bench.contraction_flops_per_scale(1024, 4, 2.0, 10)
     assert len(ana) == len(syn) == 11
     assert abs(sum(ana) / sum(syn) - 2.0) < 1e-3
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """`bench.py --impl reference` times full, unsampled CPU pairs of the
+    restatement and never loads the CUDA library (small B here)."""
+    import json
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--B', '64', '--N', '3', "
+            "'--steps', '2', '--warmup', '1']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'cuda_lib': 'libs2dw_cuda' in maps, 'oracle_lib': 'libs2dw_oracle' in maps}))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    line, libs = lines[0], lines[-1]
+    assert libs == {"cuda_lib": False, "oracle_lib": True}
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 1
+    assert line["config"]["recon_err"] < 1e-10
+    assert "unsampled" in line["cpu_baseline"]["sample"]
+    assert abs(line["ms_per_step"] * line["value"] - 1e3) < 1e-6 * 1e3
