@@ -766,6 +766,14 @@ def main():
             split["pair_roofline"] = pair_roofline(B, N, alpha, J, 1e3 / split["value"], fp64_peak)
         except Exception as ex:
             split = {"error": str(ex)[:300]}
+    # the benchmark configuration itself in the split form: one map per pair
+    split_one = None
+    if args.split_maps > 0 and rank == 0:
+        try:
+            split_one = split_stats(B, N, alpha, J, 1, repeats=10)
+            split_one["pair_roofline"] = pair_roofline(B, N, alpha, J, 1e3 / split_one["value"], fp64_peak)
+        except Exception as ex:
+            split_one = {"error": str(ex)[:300]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -775,6 +783,25 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {ex}"}
 
     if rank == 0:
+        def g(d, *ks):
+            for k in ks:
+                if not isinstance(d, dict) or k not in d:
+                    return None
+                d = d[k]
+            return d
+
+        # compact figures last: a reader of the line's tail sees them
+        summary = {
+            "fp64_pairs_s": value, "e2e_pairs_s": g(e2e, "value"), "cpu_pairs_s": g(cpu, "value"),
+            "roofline_frac_dominant_kernel": g(roofline, "frac"), "roofline_frac_pair": g(roofline, "pair", "frac"),
+            "split_one_map_pairs_s": g(split_one, "value"), "split_one_map_vs_fp64": g(split_one, "speedup_vs_fp64"),
+            "split_32maps_pairs_s_per_map": g(split, "value"), "split_32maps_vs_fp64": g(split, "speedup_vs_fp64"),
+            "split_max_w_err": g(split, "max_w_err"), "split_b256_vs_fp64": g(split_b256, "speedup_vs_fp64"),
+            "large_b2048_pairs_s": g(large, "value"), "large_split_vs_fp64": g(large, "split", "speedup_vs_fp64"),
+            "serving_rps": g(serving, "throughput_rps"), "serving_p50_ms": g(serving, "p50_ms"),
+            "serving_p99_ms": g(serving, "p99_ms"), "serving_split_p50_ms": g(serving, "split", "p50_ms"),
+            "serving_split_p99_ms": g(serving, "split", "p99_ms"),
+        }
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
@@ -786,9 +813,9 @@ def main():
                        "launch": "direct" if args.no_graph else "CUDA graph replay of the pair",
                        "l2": f"each step reads/writes a {8 * plan.wav_size / 1e6:.0f} MB wavelet array (> 126 MB L2); flm from a ring of {nring}",
                        "recon_err": recon},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
-            "split": split, "split_b256": split_b256, "large": large,
-            "gpu_launches": (la + ls) * args.steps, "kernels": kernel_ms,
+            "gpu_launches": (la + ls) * args.steps, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "kernels": kernel_ms, "large": large, "split_b256": split_b256, "split": split,
+            "split_one_map": split_one, "serving": serving, "summary": summary,
         }
         print(json.dumps(line), flush=True)
     plan.close()

@@ -1,0 +1,120 @@
+"""Oracle parity of every scale at the benchmark sizes, the full-band scales
+(bl = B, l up to B-1) included.
+
+B=1024, N=4, alpha=2, J=10: the unsampled oracle runs here, on all host
+threads (tens of seconds), and every coefficient of every scale is compared,
+for the analysis of the benchmark's seeded map and for the synthesis of
+seeded random coefficients (random, so that the synthesis is pinned as an
+operator and not only through a round trip).
+
+B=2048, N=8, alpha=2, J=11, C_l = (1/(l(l+1)))^1.2: the oracle takes tens of
+minutes there, so its outputs come from a fixture made offline by
+tests/golden/make_b2048_fixture.py: sampled (b, g) rows of every scale with
+each scale's max|w|, and sampled l-rows of the synthesis of seeded random
+coefficients with max|flm|.
+
+Tolerance: 1e-12 relative to the scale's max|w| (analysis) or to max|flm|
+(synthesis), the plain FP64 form's parity bar.  The measured errors are
+printed (pytest -s shows them).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from s2dw_b200 import core
+from s2dw_b200.workload import gaussian_flm, transform_setup
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-12
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _random_coefficients(rng, bls, N, bs):
+    wav = [np.asfortranarray(rng.standard_normal((2 * bl - 1) * 2 * bl * N).reshape((2 * bl - 1, 2 * bl, N),
+                                                                                      order="F")) for bl in bls]
+    sc = np.asfortranarray(rng.standard_normal((bs, bs)) + 1j * rng.standard_normal((bs, bs)))
+    return wav, sc
+
+
+@pytest.mark.gpu
+def test_b1024_every_scale_matches_the_unsampled_oracle():
+    B, N, alpha = 1024, 4, 2.0
+    O.set_num_threads(_threads())
+    t = transform_setup(B, N, alpha)
+    J, bs = t["J"], t["bl_scoeff"]
+    a = (t["K_gamma"], t["Slm"], J, B, N, bs, alpha)
+    s = (t["K_gamma"], t["Phi2"], t["Slm"], J, B, N, bs, alpha)
+    flm = gaussian_flm(B, seed=0)
+    wav, sc = core.s2dw_core_analysis_flm2wav_dynamic(flm, *a)
+    ref, sc_ref = O.analysis_dynamic(flm, *a)
+    errs = []
+    for j, (w, r) in enumerate(zip(wav, ref)):
+        errs.append(np.abs(w - r).max() / np.abs(r).max())
+    print("\nB=1024 N=4 analysis, max|w_gpu - w_oracle|/max|w| per scale:",
+          " ".join(f"{e:.1e}" for e in errs))
+    np.testing.assert_array_equal(sc, sc_ref)
+    assert max(errs) <= TOL, errs
+    del wav, ref
+
+    bls = [core.band_limits(j, B, alpha)[0] for j in range(J + 1)]
+    rw, rsc = _random_coefficients(np.random.default_rng(1024), bls, N, bs)
+    f = core.s2dw_core_synthesis_wav2flm_dynamic(rw, rsc, *s)
+    f_ref = O.synthesis_dynamic(rw, rsc, *s)
+    err = np.abs(f - f_ref).max() / np.abs(f_ref).max()
+    lerr = np.abs(f - f_ref).max(axis=1) / np.abs(f_ref).max()
+    print(f"B=1024 N=4 synthesis of random coefficients: max|f_gpu - f_oracle|/max|f| = {err:.1e}"
+          f" (l >= 512: {lerr[512:].max():.1e})")
+    assert err <= TOL
+
+
+def _fixture():
+    path = os.path.join(GOLD, "oracle_B2048_N8_samples.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"{path} is missing: run tests/golden/make_b2048_fixture.py")
+    return np.load(path)
+
+
+@pytest.mark.gpu
+def test_b2048_analysis_rows_match_the_oracle_fixture():
+    g = _fixture()
+    B, N, alpha, J = int(g["B"]), int(g["N"]), float(g["alpha"]), int(g["J"])
+    t = transform_setup(B, N, alpha, J)
+    flm = gaussian_flm(B, seed=0, power=float(g["power"]))
+    wav, _ = core.s2dw_core_analysis_flm2wav_dynamic(flm, t["K_gamma"], t["Slm"], J, B, N, t["bl_scoeff"], alpha)
+    errs = []
+    for j in range(J + 1):
+        rows = np.stack([wav[j][:, b, gg] for b, gg in g[f"ana_pairs_{j}"]])
+        errs.append(np.abs(rows - g[f"ana_rows_{j}"]).max() / float(g[f"ana_max_{j}"]))
+    print("\nB=2048 N=8 analysis, sampled rows, max|dw|/max|w| per scale:", " ".join(f"{e:.1e}" for e in errs))
+    assert max(errs) <= TOL, errs
+
+
+@pytest.mark.gpu
+def test_b2048_synthesis_rows_match_the_oracle_fixture():
+    sys.path.insert(0, GOLD)
+    from make_b2048_fixture import synthesis_inputs
+
+    g = _fixture()
+    B, N, alpha, J = int(g["B"]), int(g["N"]), float(g["alpha"]), int(g["J"])
+    t = transform_setup(B, N, alpha, J)
+    bls = [int(b) for b in g["bl"]]
+    wav, sc = synthesis_inputs(J, bls, t["bl_scoeff"])
+    f = core.s2dw_core_synthesis_wav2flm_dynamic(wav, sc, t["K_gamma"], t["Phi2"], t["Slm"], J, B, N,
+                                                 t["bl_scoeff"], alpha)
+    del wav
+    worst = {}
+    for l in g["syn_rows"]:
+        l = int(l)
+        worst[l] = np.abs(f[l, :l + 1] - g[f"syn_row_{l}"]).max() / float(g["syn_max"])
+    print("\nB=2048 N=8 synthesis of random coefficients, sampled l-rows, max|df|/max|f|:",
+          " ".join(f"l={k}:{v:.1e}" for k, v in worst.items()))
+    assert max(worst.values()) <= TOL, worst
