@@ -182,6 +182,8 @@ def analysis_static(flm, K, S, J, B, N, bl_scoeff, alpha):
 
 
 def synthesis_dynamic(wav, scoeff, K, Phi2, S, J, B, N, bl_scoeff, alpha):
+    if len(wav) != J + 1:
+        raise ValueError(f"oracle synthesis_dynamic: {len(wav)} scales given, J+1 = {J + 1} expected")
     flm = np.zeros((B, B), dtype=np.complex128, order="F")
     wav = [np.asfortranarray(w) for w in wav]
     ptrs = (_dp * (J + 1))(*[_p(w) for w in wav])

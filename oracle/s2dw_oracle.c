@@ -559,6 +559,8 @@ int orc_analysis_scale(int jj, double *out, size_t astride, size_t bstride, size
 int orc_analysis_dynamic(double *const *wav, dcx *scoeff, const dcx *flm, const double *K_gamma,
                          const dcx *Slm, int J, int B, int N, int bl_scoeff, double alpha)
 {
+    for (int jj = 0; jj <= J; jj++)
+        if (!wav[jj]) return ORC_ERR_MEM;
     for (int jj = 0; jj <= J; jj++) {
         int hi, lo;
         orc_band_limits(jj, B, alpha, &hi, &lo);
@@ -737,6 +739,8 @@ int orc_synthesis_dynamic(dcx *flm, double *const *wav, const dcx *scoeff, const
                           const double *Phi2, const dcx *Slm, int J, int B, int N, int bl_scoeff,
                           double alpha)
 {
+    for (int jj = 0; jj <= J; jj++)
+        if (!wav[jj]) return ORC_ERR_MEM;
     for (size_t i = 0; i < (size_t)B * B; i++) flm[i] = 0.0;
     for (int jj = 0; jj <= J; jj++) {
         int hi, lo;

@@ -109,7 +109,12 @@ void build_twiddles(int M, std::vector<double2> &hi, std::vector<double2> &lo);
 // ---------------------------------------------------------------------------
 // Transform modes.  CZT_* are chirp-z (Bluestein) transforms of any length;
 // FFT_ANA_BETA / FFT_SYN_BETA are the beta transforms as one power-of-two FFT
-// of length 4*bl (used when 4*bl is a power of two).
+// of length L = 2*bl (used when 2*bl is a power of two, bl >= 8): the analysis
+// beta sum is a DCT-III of length L (cos rows) or, on the reversed input, a
+// DST-III (i sin rows); the synthesis beta sum with its +-m' fold is the
+// matching DCT-II / DST-II.  Each runs as one complex FFT of length L with a
+// pre-twiddle, an even/odd reordering and a post-twiddle (Makhoul's
+// algorithm, complex-linear, so complex rows need no real/imaginary split).
 enum CztMode {
     CZT_ANA_BETA = 0,
     CZT_ANA_ALPHA = 1,
@@ -216,6 +221,7 @@ int launch_fprep(double2 *F, const double2 *flm, const double *Om, int B, int Bp
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
 void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread, 0 = general engine only
+void set_large_2048(bool on);  // M = 2048 transforms on the one-row-per-CTA engines (default on)
 void set_alpha_prefetch(bool on);  // synthesis alpha / analysis beta stages: persistent kernel with prefetched input (default on)
 void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels
 int launch_zero(double *p, long long n, cudaStream_t s);

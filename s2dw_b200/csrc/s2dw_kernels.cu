@@ -765,6 +765,66 @@ __device__ __forceinline__ double2 hf_at(const double2 *Hf, int k, int M)
     return Hf[k];
 }
 
+// ---- beta transforms as FFTs of length L = 2 bl (Makhoul's algorithm) ----
+// Analysis (s2dw_core_mod.f90:708-743), one row X(p), p < bl:
+//   cos rows (m+N-1 even): Y(b) = sum_p c_p X(p) cos(p beta_b), c_0 = 1, c_p = 2,
+//   sin rows (m+N-1 odd):  Y(b) = X(0) + sum_{p>=1} 2i X(p) sin(p beta_b),
+// beta_b = pi (2b+1)/(2L), b < L.  The cos sum is a DCT-III of length L:
+//   V_0 = X(0), V_k = e_k X(k) (0 < k < bl), V_bl = 0, V_k = conj(e_{L-k}) X(L-k) (k > bl),
+//   v = sum_k V_k e^{+2 pi i k n/L},  Y(2n) = v_n, Y(2n+1) = v_{L-1-n}  (n < bl),
+// e_k = exp(i pi k/(2L)) (the czt.pre table).  The sin sum is the same DCT-III
+// of the reversed input times i(-1)^b, which moves factors -i (k < bl) and +i
+// (k > bl) onto V and i, -i onto the two output halves; its V_0 is 0 and the
+// reference's m' = 0 term X(0) (eta = 1) is added to every output.
+// Synthesis (:1157-1198), one row u_b, b < L, folded over +-m':
+//   cos rows (m+n even): V'(0) = sum_b u_b, V'(m') = 2 sum_b u_b cos(m' beta_b),
+//   sin rows (m+n odd):  V'(m') = -2i sum_b u_b sin(m' beta_b),
+// a DCT-II of length L: permute v_n = u_{2n}, v_{L-1-n} = u_{2n+1} (n < bl),
+// V = sum_n v_n e^{-2 pi i k n/L}, V'(m') = conj(e_m') V_m' +- e_m' V_{L-m'}
+// (+ cos, - sin; the sin rows' input carries (-1)^b).  A sin row's V'(0)
+// multiplies d^l_{0m}(pi/2) d^l_{0n}(pi/2), which is zero for every l when m+n
+// is odd, so it is stored as 0.
+
+// Position b of the beta grid whose value sits at FFT index k in the
+// DCT-II / DCT-III reordering (k < bl: b = 2k; k >= bl: b = 2L-1-2k).
+__device__ __forceinline__ int beta_src(int k, int bl) { return k < bl ? 2 * k : 4 * bl - 1 - 2 * k; }
+
+// DCT-III input V_k of the analysis beta transform of row X (bl values).
+__device__ __forceinline__ double2 ana_beta_in(const double2 *X, int k, int bl, bool sn, const double2 *e)
+{
+    if (k == 0) return sn ? make_double2(0.0, 0.0) : X[0];
+    if (k < bl) {
+        const double2 x = cmul(X[k], e[k]);
+        return sn ? make_double2(x.y, -x.x) : x;  // -i x
+    }
+    if (k == bl) return make_double2(0.0, 0.0);
+    const int p = 2 * bl - k;
+    const double2 x = cmul(X[p], cconj(e[p]));
+    return sn ? make_double2(-x.y, x.x) : x;  // i x
+}
+
+// Output of the analysis beta transform held at FFT index j: its b, and the
+// value (the sin rows' factor i or -i and the m' = 0 term x0 applied).
+__device__ __forceinline__ double2 ana_beta_out(double2 y, int j, int bl, bool sn, double2 x0, int *b)
+{
+    if (j < bl) {
+        *b = 2 * j;
+        if (sn) y = make_double2(-y.y + x0.x, y.x + x0.y);  // i y + x0
+    } else {
+        *b = 4 * bl - 1 - 2 * j;
+        if (sn) y = make_double2(y.y + x0.x, -y.x + x0.y);  // -i y + x0
+    }
+    return y;
+}
+
+// Folded synthesis beta output V'(m') from the FFT values at m' and L-m'.
+__device__ __forceinline__ double2 syn_beta_out(double2 vk, double2 vlk, int mpv, bool sn, const double2 *e)
+{
+    if (mpv == 0) return sn ? make_double2(0.0, 0.0) : vk;
+    const double2 y = cmul(vk, cconj(e[mpv])), z = cmul(vlk, e[mpv]);
+    return sn ? csub(y, z) : cadd(y, z);
+}
+
 // Input element k of transform `row` of a MODE transform (pre-chirp or
 // pre-twiddle applied); zero outside the transform's input range.
 template <int MODE>
@@ -794,23 +854,22 @@ __device__ __forceinline__ double2 fft_load(const CztArgs &a, int row, int k, co
         double2 x = a.in_c[((size_t)g * bl + m) * bl + ab];
         if (((m + N - 1) & 1) && mpv < 0) x = make_double2(-x.x, -x.y);
         return cmul(x, a.czt.pre[k]);
-    } else if (MODE == FFT_ANA_BETA) {  // row = (g, m); k = m' mod 4bl, pre = exp(i pi m'/(4bl))
+    } else if (MODE == FFT_ANA_BETA) {  // row = (g, m); DCT-III input V_k, k < L = 2bl
         const int g = row / bl, m = row % bl;
-        if (k < bl) return cmul(a.in_c[((size_t)g * bl + m) * bl + k], a.czt.pre[k]);
-        if (k > 3 * bl) {
-            const int p = 4 * bl - k;
-            double2 x = a.in_c[((size_t)g * bl + m) * bl + p];
-            if ((m + N - 1) & 1) x = make_double2(-x.x, -x.y);
-            return cmul(x, cconj(a.czt.pre[p]));
-        }
-        return zero;
-    } else {  // CZT_SYN_BETA / FFT_SYN_BETA: row = (q, m); k = b; gamma DFT on the fly
+        return ana_beta_in(a.in_c + ((size_t)g * bl + m) * bl, k, bl, (m + N - 1) & 1, a.czt.pre);
+    } else if (MODE == FFT_SYN_BETA) {  // row = (q, m); DCT-II input: u at b = beta_src(k), gamma DFT on the fly
+        const int q = row / bl, m = row % bl, b = beta_src(k, bl);
+        double2 u = zero;
+        for (int g = 0; g < N; g++) u = cadd(u, cmul(a.in_c[((size_t)g * bl + m) * (2 * bl) + b], ph[q * N + g]));
+        u = cscale(u, a.wq[b]);
+        return (((m + a.nq[q]) & 1) && (b & 1)) ? make_double2(-u.x, -u.y) : u;
+    } else {  // CZT_SYN_BETA: row = (q, m); k = b; gamma DFT on the fly
         if (k >= 2 * bl) return zero;
         const int q = row / bl, m = row % bl;
         double2 u = zero;
         for (int g = 0; g < N; g++) u = cadd(u, cmul(a.in_c[((size_t)g * bl + m) * (2 * bl) + k], ph[q * N + g]));
         u = cscale(u, a.wq[k]);
-        return MODE == CZT_SYN_BETA ? cmul(u, a.czt.pre[k]) : u;
+        return cmul(u, a.czt.pre[k]);
     }
 }
 
@@ -874,6 +933,15 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
         for (int i = 0; i < V; i++) {
             const int pos = pos_of<V>(i, RL, t, lgM), r = pos >> lgM, b = pos & (M - 1), row = row0 + r;
             if (row >= a.rows || b >= Bout) continue;
+            if (MODE == FFT_ANA_BETA) {
+                const int g = row / bl, m = row % bl;
+                const bool sn = (m + N - 1) & 1;
+                const double2 *X = a.in_c + ((size_t)g * bl + m) * bl;
+                int bo;
+                const double2 y = ana_beta_out(v[i], b, bl, sn, sn ? X[0] : make_double2(0.0, 0.0), &bo);
+                a.out_c[((size_t)g * bl + m) * (2 * bl) + bo] = y;
+                continue;
+            }
             const double2 y = CHIRP ? cmul(v[i], a.czt.post[b]) : v[i];
             if (MODE == CZT_ANA_ALPHA) {
                 const int g = row / bl, bp = row % bl;
@@ -917,13 +985,13 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
             const int t0 = bl - 1 + mpv, t1 = bl - 1 - mpv;
             y = cmul(buf[padix((r << lgM) + t0)], a.czt.post[t0]);
             z = cmul(buf[padix((r << lgM) + t1)], a.czt.post[t1]);
-        } else {  // V2(m') = exp(-i pi m'/(4bl)) Z(m' mod 4bl)
-            y = cmul(buf[padix((r << lgM) + mpv)], cconj(a.czt.pre[mpv]));
-            z = (mpv > 0) ? cmul(buf[padix((r << lgM) + M - mpv)], a.czt.pre[mpv]) : make_double2(0.0, 0.0);
-        }
-        if (mpv > 0) {
-            if ((m + a.nq[q]) & 1) z = make_double2(-z.x, -z.y);
-            y = cadd(y, z);
+            if (mpv > 0) {
+                if ((m + a.nq[q]) & 1) z = make_double2(-z.x, -z.y);
+                y = cadd(y, z);
+            }
+        } else {
+            y = syn_beta_out(buf[padix((r << lgM) + mpv)], buf[padix((r << lgM) + ((M - mpv) & (M - 1)))], mpv,
+                             (m + a.nq[q]) & 1, a.czt.pre);
         }
         a.out_c[((size_t)q * bl + m) * a.out_stride + mpv] = y;
     }
@@ -991,12 +1059,49 @@ __device__ __forceinline__ void pass2x8(double2 (&v)[16], int t, const double2 *
     }
 }
 
+// Radix-8 pass for LGM = 11 (the remainder of 11 = 4+4+3), 2 butterflies per thread.
+template <int LGM, int LNS, int SIGN>
+__device__ __forceinline__ void pass8x2(double2 (&v)[16], int t, const double2 *twh, const double2 *twl)
+{
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        if (LNS > 0) {
+            const int j = (t * 2 + u) & ((1 << (LGM - 3)) - 1), k = j & ((1 << LNS) - 1);
+            double2 w = twid(twh, twl, k << (LGM - LNS - 3));
+            if (SIGN > 0) w = cconj(w);
+            const double2 w2 = cmul(w, w), w3 = cmul(w2, w), w4 = cmul(w2, w2);
+            v[8 * u + 1] = cmul(v[8 * u + 1], w);
+            v[8 * u + 2] = cmul(v[8 * u + 2], w2);
+            v[8 * u + 3] = cmul(v[8 * u + 3], w3);
+            v[8 * u + 4] = cmul(v[8 * u + 4], w4);
+            v[8 * u + 5] = cmul(v[8 * u + 5], cmul(w4, w));
+            v[8 * u + 6] = cmul(v[8 * u + 6], cmul(w4, w2));
+            v[8 * u + 7] = cmul(v[8 * u + 7], cmul(w4, w3));
+        }
+        Dft<8, SIGN>::run(&v[8 * u]);
+    }
+}
+
+// Radix of the first pass of the forward (SIGN < 0) or inverse (SIGN > 0)
+// transform of size 2^LGM, and of its last pass.
+template <int LGM, int SIGN>
+__host__ __device__ constexpr int first_radix()
+{
+    return SIGN < 0 ? 16 : (LGM == 13 ? 2 : LGM == 11 ? 8 : 16);
+}
+template <int LGM, int SIGN>
+__host__ __device__ constexpr int last_radix()
+{
+    return SIGN > 0 ? 16 : (LGM == 13 ? 2 : LGM == 11 ? 8 : 16);
+}
+
 // Shared-memory exchange after a pass of radix R at LNS into the input
 // positions of the next pass of radix RN (values per thread: 16).
 template <int LGM, int R, int LNS, int RN>
 __device__ __forceinline__ void exchange(double2 (&v)[16], double2 *buf, int t)
 {
-    constexpr int NB = 16 / R, LR = (R == 16 ? 4 : 1), NBN = 16 / RN, LRN = (RN == 16 ? 4 : 1);
+    constexpr int NB = 16 / R, LR = (R == 16 ? 4 : R == 8 ? 3 : 1), NBN = 16 / RN,
+                  LRN = (RN == 16 ? 4 : RN == 8 ? 3 : 1);
 #pragma unroll
     for (int u = 0; u < NB; u++) {
         const int j = t * NB + u;
@@ -1021,7 +1126,19 @@ template <int LGM, int SIGN>
 __device__ __forceinline__ void fft_large(double2 (&v)[16], double2 *buf, int t, const double2 *twh,
                                           const double2 *twl)
 {
-    if (LGM == 12) {
+    if (LGM == 11 && SIGN < 0) {  // forward: 16,16,8
+        pass16<11, 0, SIGN>(v, t, twh, twl);
+        exchange<11, 16, 0, 16>(v, buf, t);
+        pass16<11, 4, SIGN>(v, t, twh, twl);
+        exchange<11, 16, 4, 8>(v, buf, t);
+        pass8x2<11, 8, SIGN>(v, t, twh, twl);
+    } else if (LGM == 11) {  // inverse: 8,16,16
+        pass8x2<11, 0, SIGN>(v, t, twh, twl);
+        exchange<11, 8, 0, 16>(v, buf, t);
+        pass16<11, 3, SIGN>(v, t, twh, twl);
+        exchange<11, 16, 3, 16>(v, buf, t);
+        pass16<11, 7, SIGN>(v, t, twh, twl);
+    } else if (LGM == 12) {
         pass16<12, 0, SIGN>(v, t, twh, twl);
         exchange<12, 16, 0, 16>(v, buf, t);
         pass16<12, 4, SIGN>(v, t, twh, twl);
@@ -1052,19 +1169,20 @@ template <int LGM, int R>
 __device__ __forceinline__ int lpos(int t, int i)
 {
     if (R == 16) return t + (i << (LGM - 4));
+    if (R == 8) return ((t * 2 + (i >> 3)) & ((1 << (LGM - 3)) - 1)) + ((i & 7) << (LGM - 3));
     const int u = i >> 1, s = i & 1;
     return ((t * 8 + u) & ((1 << (LGM - 1)) - 1)) + (s << (LGM - 1));
 }
 
 template <int MODE, int LGM>
-__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_large_kernel(CztArgs a)
+__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 2 : 1)) fft_large_kernel(CztArgs a)
 {
     constexpr int M = 1 << LGM, THREADS = M / 16;
     constexpr bool CHIRP = (MODE != FFT_ANA_BETA && MODE != FFT_SYN_BETA);
     constexpr bool SYNB = (MODE == CZT_SYN_BETA || MODE == FFT_SYN_BETA);
     // first-pass radix of the transform run first, last-pass radix of the last
-    constexpr int R0 = (LGM == 13 && MODE == FFT_ANA_BETA) ? 2 : 16;
-    constexpr int RL = (LGM == 13 && MODE == FFT_SYN_BETA) ? 2 : 16;
+    constexpr int R0 = MODE == FFT_ANA_BETA ? first_radix<LGM, +1>() : first_radix<LGM, -1>();
+    constexpr int RL = MODE == FFT_SYN_BETA ? last_radix<LGM, -1>() : last_radix<LGM, +1>();
     extern __shared__ double2 smem[];
     double2 *buf = smem;
     double2 *twh = smem + padix(M) + 1;
@@ -1114,22 +1232,20 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
                 if (((rr + N - 1) & 1) && mpv < 0) x = make_double2(-x.x, -x.y);
                 x = cmul(x, a.czt.pre[k]);
             }
-        } else if (MODE == FFT_ANA_BETA) {  // (g, m = rr), k = m' mod 4bl
-            if (k < bl) {
-                x = cmul(a.in_c[((size_t)g * bl + rr) * bl + k], a.czt.pre[k]);
-            } else if (k > 3 * bl) {
-                const int pp = 4 * bl - k;
-                x = a.in_c[((size_t)g * bl + rr) * bl + pp];
-                if ((rr + N - 1) & 1) x = make_double2(-x.x, -x.y);
-                x = cmul(x, cconj(a.czt.pre[pp]));
-            }
-        } else {  // synthesis beta, (q = g, m = rr), k = b
+        } else if (MODE == FFT_ANA_BETA) {  // (g, m = rr), DCT-III input
+            x = ana_beta_in(a.in_c + ((size_t)g * bl + rr) * bl, k, bl, (rr + N - 1) & 1, a.czt.pre);
+        } else if (MODE == FFT_SYN_BETA) {  // (q = g, m = rr), DCT-II input at b = beta_src(k)
+            const int b = beta_src(k, bl);
+            double2 u = zero;
+            for (int gg = 0; gg < N; gg++) u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + b], ph[gg]));
+            x = cscale(u, a.wq[b]);
+            if (((rr + a.nq[g]) & 1) && (b & 1)) x = make_double2(-x.x, -x.y);
+        } else {  // CZT_SYN_BETA, (q = g, m = rr), k = b
             if (k < 2 * bl) {
                 double2 u = zero;
                 for (int gg = 0; gg < N; gg++)
                     u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + k], ph[gg]));
-                x = cscale(u, a.wq[k]);
-                if (MODE == CZT_SYN_BETA) x = cmul(x, a.czt.pre[k]);
+                x = cmul(cscale(u, a.wq[k]), a.czt.pre[k]);
             }
         }
         v[i] = x;
@@ -1141,7 +1257,7 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
         fft_large<LGM, -1>(v, buf, t, twh, twl);
     } else {
         fft_large<LGM, -1>(v, buf, t, twh, twl);
-        constexpr int RF = (LGM == 13) ? 2 : 16;
+        constexpr int RF = last_radix<LGM, -1>();
 #pragma unroll
         for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<MODE>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
         fft_large<LGM, +1>(v, buf, t, twh, twl);
@@ -1152,6 +1268,14 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
         for (int i = 0; i < 16; i++) {
             const int b = lpos<LGM, RL>(t, i);
             if (b >= Bout) continue;
+            if (MODE == FFT_ANA_BETA) {
+                const bool sn = (rr + N - 1) & 1;
+                const double2 *X = a.in_c + ((size_t)g * bl + rr) * bl;
+                int bo;
+                const double2 y = ana_beta_out(v[i], b, bl, sn, sn ? X[0] : zero, &bo);
+                a.out_c[((size_t)g * bl + rr) * (2 * bl) + bo] = y;
+                continue;
+            }
             const double2 y = CHIRP ? cmul(v[i], a.czt.post[b]) : v[i];
             if (MODE == CZT_ANA_ALPHA) {
                 double *p = a.out_r + (size_t)b + (size_t)n * (2 * rr + (size_t)2 * bl * g);
@@ -1180,18 +1304,17 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_larg
         return;
     }
     for (int mpv = t; mpv < bl; mpv += THREADS) {
-        double2 y, z;
+        double2 y;
         if (MODE == CZT_SYN_BETA) {
             const int t0 = bl - 1 + mpv, t1 = bl - 1 - mpv;
             y = cmul(buf[padix(t0)], a.czt.post[t0]);
-            z = cmul(buf[padix(t1)], a.czt.post[t1]);
+            double2 z = cmul(buf[padix(t1)], a.czt.post[t1]);
+            if (mpv > 0) {
+                if ((rr + a.nq[g]) & 1) z = make_double2(-z.x, -z.y);
+                y = cadd(y, z);
+            }
         } else {
-            y = cmul(buf[padix(mpv)], cconj(a.czt.pre[mpv]));
-            z = (mpv > 0) ? cmul(buf[padix(M - mpv)], a.czt.pre[mpv]) : zero;
-        }
-        if (mpv > 0) {
-            if ((rr + a.nq[g]) & 1) z = make_double2(-z.x, -z.y);
-            y = cadd(y, z);
+            y = syn_beta_out(buf[padix(mpv)], buf[padix((M - mpv) & (M - 1))], mpv, (rr + a.nq[g]) & 1, a.czt.pre);
         }
         a.out_c[((size_t)g * bl + rr) * a.out_stride + mpv] = y;
     }
@@ -1240,12 +1363,12 @@ __device__ __forceinline__ void pf_prefetch(const CztArgs &a, int r, double2 *st
 }
 
 template <int MODE, int LGM>
-__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_kernel(CztArgs a)
+__global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 2 : 1)) fft_pf_kernel(CztArgs a)
 {
     static_assert(MODE == CZT_SYN_ALPHA || MODE == FFT_ANA_BETA, "contiguous-input stages only");
     constexpr int M = 1 << LGM, THREADS = M / 16;
     // first-pass radix of the transform run first (as fft_large_kernel)
-    constexpr int R0 = (LGM == 13 && MODE == FFT_ANA_BETA) ? 2 : 16;
+    constexpr int R0 = MODE == FFT_ANA_BETA ? first_radix<LGM, +1>() : first_radix<LGM, -1>();
     extern __shared__ double2 smem[];
     double2 *buf = smem;
     double2 *twh = smem + padix(M) + 1;
@@ -1265,6 +1388,8 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_k
         pf_wait_all();
         __syncthreads();  // row r staged; the previous row's reads of buf done
         double2 v[16];
+        bool sn = false;     // FFT_ANA_BETA: sin row
+        double2 x0 = zero;   // FFT_ANA_BETA: the row's X(0)
         if (MODE == CZT_SYN_ALPHA) {
             const double *sd = reinterpret_cast<const double *>(stg);
 #pragma unroll
@@ -1272,22 +1397,11 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_k
                 const int k = lpos<LGM, R0>(t, i);
                 v[i] = (k < n) ? cmul(make_double2(sd[k], sd[n + k]), a.czt.pre[k]) : zero;
             }
-        } else {  // k = m' mod 4bl, as fft_large_kernel's FFT_ANA_BETA load
-            const bool flip = (rr + N - 1) & 1;
+        } else {  // DCT-III input, as fft_large_kernel's FFT_ANA_BETA load
+            sn = (rr + N - 1) & 1;
+            x0 = stg[0];
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const int k = lpos<LGM, R0>(t, i);
-                double2 x = zero;
-                if (k < bl) {
-                    x = cmul(stg[k], a.czt.pre[k]);
-                } else if (k > 3 * bl) {
-                    const int pp = 4 * bl - k;
-                    x = stg[pp];
-                    if (flip) x = make_double2(-x.x, -x.y);
-                    x = cmul(x, cconj(a.czt.pre[pp]));
-                }
-                v[i] = x;
-            }
+            for (int i = 0; i < 16; i++) v[i] = ana_beta_in(stg, lpos<LGM, R0>(t, i), bl, sn, a.czt.pre);
         }
         __syncthreads();  // staging free: copy the next row while this one runs
         if (r + (int)gridDim.x < rows) pf_prefetch<MODE, THREADS>(a, r + gridDim.x, stg, t);
@@ -1295,7 +1409,7 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_k
 
         if (MODE == CZT_SYN_ALPHA) {
             fft_large<LGM, -1>(v, buf, t, twh, twl);
-            constexpr int RF = (LGM == 13) ? 2 : 16;
+            constexpr int RF = last_radix<LGM, -1>();
 #pragma unroll
             for (int i = 0; i < 16; i++) v[i] = cmul(v[i], hf_at<MODE>(a.czt.Hf, lpos<LGM, RF>(t, i), M));
             fft_large<LGM, +1>(v, buf, t, twh, twl);
@@ -1316,8 +1430,9 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 12 ? 2 : 1)) fft_pf_k
             fft_large<LGM, +1>(v, buf, t, twh, twl);
 #pragma unroll
             for (int i = 0; i < 16; i++) {
-                const int b = lpos<LGM, 16>(t, i);
-                if (b < Bout) a.out_c[((size_t)g * bl + rr) * (2 * bl) + b] = v[i];
+                int b;
+                const double2 y = ana_beta_out(v[i], lpos<LGM, 16>(t, i), bl, sn, x0, &b);
+                a.out_c[((size_t)g * bl + rr) * (2 * bl) + b] = y;
             }
         }
     }
@@ -1615,6 +1730,7 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
 }
 
 static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
+static bool g_large_2048 = true;  // M = 2048 transforms on the one-row-per-CTA engines
 static bool g_alpha_prefetch = true;  // contiguous-input stages: persistent kernel with prefetched input
 
 // Persistent launch of the prefetching stages: as many CTAs as fit on the
@@ -1662,13 +1778,15 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
         // 256-bit loads (the chirp-table loads from L2, not the input,
         // dominate its remaining memory stalls).
         if (g_alpha_prefetch && a.mode == CZT_SYN_ALPHA && ((uintptr_t)a.in_r & 15) == 0) {
+            if (M == 2048 && g_large_2048) return launch_pf<CZT_SYN_ALPHA, 11>(a, s);
             if (M == 4096) return launch_pf<CZT_SYN_ALPHA, 12>(a, s);
             if (M == 8192) return launch_pf<CZT_SYN_ALPHA, 13>(a, s);
         }
         if (g_alpha_prefetch && a.mode == FFT_ANA_BETA && ((uintptr_t)a.in_c & 15) == 0) {
+            if (M == 2048 && g_large_2048) return launch_pf<FFT_ANA_BETA, 11>(a, s);
             if (M == 4096) return launch_pf<FFT_ANA_BETA, 12>(a, s);
-            if (M == 8192) return launch_pf<FFT_ANA_BETA, 13>(a, s);
         }
+        if (M == 2048 && g_large_2048) return launch_large<11>(a, s);
         if (M == 4096) return launch_large<12>(a, s);
         if (M == 8192) return launch_large<13>(a, s);
     }
@@ -1677,6 +1795,7 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
 }
 
 void set_fft_values(int v) { g_fft_values = (v == 16) ? 16 : (v == 0 ? 0 : 8); }
+void set_large_2048(bool on) { g_large_2048 = on; }
 
 int launch_combine(const CombineArgs &a, cudaStream_t s)
 {

@@ -310,25 +310,27 @@ int plan_build(s2dwc_plan *p)
                     p->tw[c.M] = tw;
                 }
             }
-            const int L4 = 4 * b;
-            if (L4 >= 16 && L4 <= 8192 && (L4 & (L4 - 1)) == 0) {
-                std::vector<double2> tw4;
-                build_beta_twiddles(b, tw4);
+            // beta transforms as one power-of-two FFT of length L = 2 bl (a
+            // DCT-III / DCT-II pair of that length) when 2 bl is a power of two
+            const int L2 = 2 * b;
+            if (L2 >= 16 && L2 <= 4096 && (L2 & (L2 - 1)) == 0) {
+                std::vector<double2> twb;
+                build_beta_twiddles(b, twb);
                 for (int md : {(int)FFT_ANA_BETA, (int)FFT_SYN_BETA}) {
                     CztDev d;
-                    d.M = L4;
-                    d.spec = CztSpec{md == FFT_ANA_BETA ? 4 * b : 2 * b, md == FFT_ANA_BETA ? 2 * b : 2 * b - 1,
-                                     L4, md == FFT_ANA_BETA ? 1 : -1, 0, 0, L4};
-                    if ((st = dev_upload(p, &d.pre, tw4))) return st;
+                    d.M = L2;
+                    d.spec = CztSpec{2 * b, md == FFT_ANA_BETA ? 2 * b : 2 * b - 1, L2, md == FFT_ANA_BETA ? 1 : -1, 0,
+                                     0, L2};
+                    if ((st = dev_upload(p, &d.pre, twb))) return st;
                     arr[md] = d;
                 }
-                if (!p->tw.count(L4)) {
+                if (!p->tw.count(L2)) {
                     std::vector<double2> hi, lo;
-                    build_twiddles(L4, hi, lo);
+                    build_twiddles(L2, hi, lo);
                     TwDev tw;
-                    tw.M = L4;
+                    tw.M = L2;
                     if ((st = dev_upload(p, &tw.hi, hi)) || (st = dev_upload(p, &tw.lo, lo))) return st;
-                    p->tw[L4] = tw;
+                    p->tw[L2] = tw;
                 }
             }
             it = by_bl.emplace(b, arr).first;
@@ -1204,6 +1206,10 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         return set_error(S2DWC_ERROR_ARG_INVALID, "device %d out of range (%d devices)", device, ndev);
     DeviceGuard dg(device);
     if (const char *fv = getenv("S2DW_FFT_VALUES")) set_fft_values(atoi(fv));
+    {
+        const char *l2 = getenv("S2DW_LARGE_2048");
+        set_large_2048(l2 ? atoi(l2) != 0 : true);
+    }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");
         set_alpha_prefetch(ap ? atoi(ap) != 0 : true);

@@ -58,7 +58,12 @@ def test_b1024_every_scale_matches_the_unsampled_oracle():
     ref, sc_ref = O.analysis_dynamic(flm, *a)
     errs = []
     for j, (w, r) in enumerate(zip(wav, ref)):
-        errs.append(np.abs(w - r).max() / np.abs(r).max())
+        scale = np.abs(r).max()
+        if scale == 0:  # a scale with an empty l range: both all zero
+            assert np.abs(w).max() == 0, f"scale {j}"
+            errs.append(0.0)
+        else:
+            errs.append(np.abs(w - r).max() / scale)
     print("\nB=1024 N=4 analysis, max|w_gpu - w_oracle|/max|w| per scale:",
           " ".join(f"{e:.1e}" for e in errs))
     np.testing.assert_array_equal(sc, sc_ref)
@@ -67,7 +72,9 @@ def test_b1024_every_scale_matches_the_unsampled_oracle():
 
     bls = [core.band_limits(j, B, alpha)[0] for j in range(J + 1)]
     rw, rsc = _random_coefficients(np.random.default_rng(1024), bls, N, bs)
-    f = core.s2dw_core_synthesis_wav2flm_dynamic(rw, rsc, *s)
+    # the library's dynamic synthesis consumes its list (as the reference
+    # frees wavdyn), so it gets a copy of the list
+    f = core.s2dw_core_synthesis_wav2flm_dynamic(list(rw), rsc, *s)
     f_ref = O.synthesis_dynamic(rw, rsc, *s)
     err = np.abs(f - f_ref).max() / np.abs(f_ref).max()
     lerr = np.abs(f - f_ref).max(axis=1) / np.abs(f_ref).max()
