@@ -249,9 +249,20 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
                        double *five, double *six);
 
 /* Synchronises with the device and reports S2DWC_ERROR_CUDA if a split-form
- * kernel gave up waiting on its tensor-core pipeline (each wait is bounded
- * by 2 s); S2DWC_OK otherwise. */
+ * kernel gave up waiting on its tensor-core pipeline since the last check
+ * (the flag is cleared when reported); S2DWC_OK otherwise.  The outputs of
+ * the calls that gave up are unspecified.  Failure detection of the kind
+ * the reference's s2dw_error reports (src/mod/s2dw_error_mod.f90:127-191),
+ * as a status instead of a halt. */
 int s2dwc_plan_check(s2dwc_plan *plan);
+
+/* Bound, in nanoseconds, on every wait of the split-form kernels' pipeline
+ * (default 2 s).  A kernel whose wait runs out stops its work, lets its own
+ * copies and tensor-core operations in flight finish, frees its tensor
+ * memory and returns; s2dwc_plan_check then reports it.  A limit too short
+ * for the pipeline's hand-offs (0 gives up on the first wait that is not
+ * already satisfied) exercises that path in tests. */
+int s2dwc_plan_set_wait_limit(s2dwc_plan *plan, long long ns);
 
 /* Analysis on device memory that allocates nothing.  This entry point has no
  * counterpart in the reference.  It computes what s2dwc_plan_analysis

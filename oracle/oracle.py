@@ -47,6 +47,8 @@ def lib():
         L.orc_init_directionality.argtypes = [_dp, ctypes.c_int, ctypes.c_int]
         L.orc_admiss.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
         L.orc_dl_beta_operator.argtypes = [_dp, ctypes.c_double, ctypes.c_int]
+        L.orc_dl_edge_ld.argtypes = [_dp, ctypes.c_int]
+        L.orc_set_dl_method.argtypes = [ctypes.c_int]
         L.orc_analysis_scale.argtypes = [ctypes.c_int, _dp, ctypes.c_size_t, ctypes.c_size_t,
                                          ctypes.c_size_t, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
@@ -140,6 +142,21 @@ def dl_plane(l, beta=np.pi / 2):
     D = np.zeros((2 * l + 1, 2 * l + 1), order="F")
     lib().orc_dl_beta_operator(_p(D), float(beta), int(l))
     return D
+
+
+def dl_plane_accurate(l):
+    """d^l(pi/2) from the long-double edge recurrence (a diagnostic, not the
+    reference's algorithm), laid out as dl_plane."""
+    D = np.zeros((2 * l + 1, 2 * l + 1), order="F")
+    lib().orc_dl_edge_ld(_p(D), int(l))
+    return D
+
+
+def set_dl_method(m):
+    """0: the reference's Turok-Bucher planes (default); 1: the accurate
+    long-double planes of dl_plane_accurate, to measure how much of a
+    difference at large l is the reference's own d-plane error."""
+    lib().orc_set_dl_method(int(m))
 
 
 def analysis_scale(jj, flm, K, S, J, B, N, alpha, debug=False):

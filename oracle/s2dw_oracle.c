@@ -379,6 +379,54 @@ void orc_dl_beta_operator(double *dl, double beta, int l)
     orc_dl_fill(dl, l);
 }
 
+/* DIAGNOSTIC, not the reference's algorithm: the plane d^l(pi/2) from the
+ * three-term recurrence in the second index at fixed first index a,
+ *   sqrt((l+b)(l-b+1)) d_{a,b-1} + sqrt((l-b)(l+b+1)) d_{a,b+1} = -2a d_{a,b},
+ * walked in long double from the closed-form edge d^l_{a,l} = sqrt(C(2l,l+a))/2^l
+ * (the edge values by exact ratios from 2^-l) down to b = 0, then
+ * d^l_{a,-b} = (-1)^(l+a) d^l_{a,b}.  Walking inward from the edge follows the
+ * dominant solution, so the planes stay within ~1e-17 of 50-digit values up
+ * to l = 2047, where the reference's Turok-Bucher planes reach 1.4e-13.
+ * Selected with orc_set_dl_method(1) to separate, in a comparison at large l,
+ * the reference algorithm's own d-plane error from the rest. */
+static int orc_dl_method = 0;
+void orc_set_dl_method(int m) { orc_dl_method = m; }
+
+void orc_dl_edge_ld(double *dl, int l)
+{
+    const size_t w = (size_t)(2 * l + 1);
+    long double *r = (long double *)malloc(sizeof(long double) * (size_t)(2 * l + 3));
+    long double *E = (long double *)malloc(sizeof(long double) * (size_t)(2 * l + 1));
+    if (!r || !E) { free(r); free(E); return; }
+    for (int b = -l; b <= l + 1; b++) r[b + l] = sqrtl((long double)(l + b) * (long double)(l - b + 1));
+    E[2 * l] = ldexpl(1.0L, -l);  /* a = l: sqrt(C(2l,2l)) / 2^l */
+    for (int a = l; a > -l; a--)  /* C(2l,l+a-1) = C(2l,l+a) (l+a)/(l-a+1) */
+        E[a - 1 + l] = E[a + l] * sqrtl((long double)(l + a) / (long double)(l - a + 1));
+    for (int a = -l; a <= l; a++) {
+        long double dn = 0.0L, d = E[a + l];
+        dl[(size_t)(a + l) + w * (size_t)(2 * l)] = (double)d;
+        for (int b = l; b >= 1; b--) {
+            const long double dm = (-2.0L * a * d - r[b + 1 + l] * dn) / r[b + l];
+            dl[(size_t)(a + l) + w * (size_t)(b - 1 + l)] = (double)dm;
+            dn = d;
+            d = dm;
+        }
+        const double sg = ((l + a) & 1) ? -1.0 : 1.0;
+        for (int b = 1; b <= l; b++)
+            dl[(size_t)(a + l) + w * (size_t)(l - b)] = sg * dl[(size_t)(a + l) + w * (size_t)(l + b)];
+    }
+    free(r);
+    free(E);
+}
+
+/* The d(pi/2) plane the transforms use: the reference's Turok-Bucher plane
+ * unless the diagnostic method is selected. */
+static void orc_dl_plane(double *dl, int l)
+{
+    if (orc_dl_method == 1) orc_dl_edge_ld(dl, l);
+    else orc_dl_beta_operator(dl, ORC_PION2, l);
+}
+
 /* ------------------------------------------------------------------ */
 /* FFT with FFTW's c2r / r2c semantics (the reference calls FFTW3's    */
 /* dfftw_plan_dft_c2r_1d / r2c_1d at s2dw_core_mod.f90:511-526 and     */
@@ -458,7 +506,7 @@ int orc_analysis_scale(int jj, double *out, size_t astride, size_t bstride, size
         double *dl = (double *)malloc(sizeof(double) * (size_t)(2 * bl + 1) * (2 * bl + 1));
 #pragma omp for schedule(dynamic, 10)
         for (int el = bl_lo + 1; el <= bl_hi - 1; el++) {
-            orc_dl_beta_operator(dl, ORC_PION2, el);
+            orc_dl_plane(dl, el);
             const size_t w = (size_t)(2 * el + 1);
 #define D(i, k) dl[((i) + el) + w * ((k) + el)]
             int kmax = (N - 1) < el ? (N - 1) : el;
@@ -682,7 +730,7 @@ int orc_synthesis_scale(int jj, dcx *flm, const double *in, size_t astride, size
         double *dl = (double *)malloc(sizeof(double) * (size_t)(2 * bl + 1) * (2 * bl + 1));
 #pragma omp for schedule(dynamic, 10)
         for (int el = bl_lo + 1; el <= bl_hi - 1; el++) {
-            orc_dl_beta_operator(dl, ORC_PION2, el);
+            orc_dl_plane(dl, el);
             const size_t w = (size_t)(2 * el + 1);
 #define D(i, k) dl[((i) + el) + w * ((k) + el)]
             int kmax = (N - 1) < el ? (N - 1) : el;

@@ -255,6 +255,7 @@ struct SplitArgs {
     const int2 *tiles;         // (m, chain tile)
     int ntiles;
     int *err;                  // set to 1 when a wait gave up
+    unsigned long long wait_ns;  // bound on every pipeline wait (the plan's wait limit)
 };
 
 struct FdigArgs {
@@ -283,6 +284,7 @@ struct SplitSynArgs {
     const int2 *tiles;         // (m, 128-row l tile)
     int ntiles;
     int *err;
+    unsigned long long wait_ns;
 };
 
 struct VdigArgs {

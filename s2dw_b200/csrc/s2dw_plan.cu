@@ -116,6 +116,7 @@ struct s2dwc_plan {
     int sp_cap = 0;
     long long sp_tg_map = 0, sp_v2f_map = 0;
     int *sp_err = nullptr;
+    unsigned long long sp_wait_ns = 2000000000ull;  // bound on every split-kernel pipeline wait (2 s)
     // moments of the coefficients (built on first use): 32 maps per pass
     double *st_part = nullptr, *st_mean = nullptr;
     int *st_flags = nullptr;
@@ -976,6 +977,7 @@ int run_analysis_split(s2dwc_plan *p, int nmaps, double *d_wav, double2 *d_scoef
             a.tiles = S.tiles;
             a.ntiles = S.ntiles;
             a.err = p->sp_err;
+            a.wait_ns = p->sp_wait_ns;
             {
                 KernelTimer kt(p, S2DWC_KIND_LWALK, sj);
                 if ((st2 = launch_split(a, sj))) return st2;
@@ -1107,6 +1109,7 @@ int run_synthesis_split(s2dwc_plan *p, int nmaps, double2 *d_flm, const double *
             b.tiles = S.stiles;
             b.ntiles = S.sntiles;
             b.err = p->sp_err;
+            b.wait_ns = p->sp_wait_ns;
             KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
             return launch_split_syn(b, sj);
         });
@@ -1649,7 +1652,21 @@ int s2dwc_plan_check(s2dwc_plan *p)
     DeviceGuard dg(p->device);
     int h = 0;
     S2DW_CUDA_TRY(cudaMemcpy(&h, p->sp_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h) return set_error(S2DWC_ERROR_CUDA, "a split-form kernel gave up waiting for its tensor-core pipeline");
+    if (h) {
+        // reported once: the flag is cleared so that later calls start clean
+        S2DW_CUDA_TRY(cudaMemset(p->sp_err, 0, sizeof(int)));
+        return set_error(S2DWC_ERROR_CUDA, "a split-form kernel gave up waiting for its tensor-core pipeline");
+    }
+    return S2DWC_OK;
+    S2DW_API_CATCH
+}
+
+int s2dwc_plan_set_wait_limit(s2dwc_plan *p, long long ns)
+{
+    S2DW_API_TRY
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_set_wait_limit: null plan");
+    if (ns < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_set_wait_limit: negative limit %lld", ns);
+    p->sp_wait_ns = ns == 0 ? 0ull : (unsigned long long)ns;
     return S2DWC_OK;
     S2DW_API_CATCH
 }

@@ -360,7 +360,18 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 __device__ __forceinline__ void cp_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on every wait
+// After a wait gave up, the issuer waits for its own bulk copies and MMAs
+// still in flight before the CTA tears down (shared memory reuse, TMEM
+// deallocation); those complete in microseconds, this bounds the wait.
+constexpr unsigned long long DRAIN_NS = 100000000ull;  // 100 ms
+// Bounded wait that ignores the abort flag (the drain after an abort).
+__device__ __forceinline__ void drain_wait(uint32_t bar, uint32_t parity)
+{
+    if (mbar_try(bar, parity)) return;
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(bar, parity) && gtimer() - t0 <= DRAIN_NS) {
+    }
+}
 
 // ---------------------------------------------------------------------------
 // dexp_kernel: exponent of max_{l in (blo, bl)} |v(l; m', m, n_q)| per
@@ -514,7 +525,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         const unsigned long long t0 = gtimer();
         while (true) {
             if (mbar_try(bar, parity)) return true;
-            if (*sAbort || gtimer() - t0 > WAIT_NS) {
+            if (*sAbort || gtimer() - t0 > a.wait_ns) {
                 *sAbort = 1;
                 return false;
             }
@@ -686,11 +697,15 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         cp_wait_all();
     } else if (lane == 0 && nout > 0) {
         // ================= issuer =================
+        // copies issued into / consumed from each map stage, last MMA commit:
+        // what the drain after an abort must wait for
+        int ncopy[S::MAP_ST] = {}, nused[S::MAP_ST] = {}, last_commit = -1;
         auto map_copy = [&](int c) {
             const int st = (c - c_start) % S::MAP_ST;
             mbar_expect_tx(full(st), DIG * B_TILE);
             bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE),
                      a.fdig + ((size_t)m * a.nch + (c - a.c0)) * DIG * B_TILE, DIG * B_TILE, full(st));
+            ncopy[st]++;
         };
         const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
                        idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
@@ -707,6 +722,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
             const int gs = k & 1, ms = k % S::MAP_ST, c = c_start + k;
             if (!wait(cutb(gs), (k >> 1) & 1)) continue;
             if (!wait(full(ms), (k / S::MAP_ST) & 1)) continue;
+            nused[ms]++;
             tc_fence_after();
             const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
             const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + ms * DIG * B_TILE), COLS * 16, 128);
@@ -723,12 +739,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
                     first_lev[lev] = false;
                 }
             mma_commit(done(gs));
+            last_commit = k;
             if (k + 2 < nout) {
                 if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
                 map_copy(c + 2);
             }
         }
-        wait(done((nout - 1) & 1), ((nout - 1) >> 1) & 1);
+        if (!wait(done((nout - 1) & 1), ((nout - 1) >> 1) & 1)) {
+            // a wait gave up: let this CTA's copies and MMAs in flight finish
+            // before its shared memory and TMEM are released.  At most one
+            // copy per stage is unconsumed; the commit of chunk k is phase
+            // k/2 of done(k%2).
+            for (int st = 0; st < S::MAP_ST; st++)
+                if (ncopy[st] > nused[st]) drain_wait(full(st), (ncopy[st] - 1) & 1);
+            if (last_commit >= 0) drain_wait(done(last_commit & 1), (last_commit >> 1) & 1);
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -954,7 +979,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArg
         const unsigned long long t0 = gtimer();
         while (true) {
             if (mbar_try(bar, parity)) return true;
-            if (*sAbort || gtimer() - t0 > WAIT_NS) {
+            if (*sAbort || gtimer() - t0 > a.wait_ns) {
                 *sAbort = 1;
                 return false;
             }
@@ -1066,10 +1091,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArg
         cp_wait_all();
     } else if (warp == ISSUER_WARP && lane == 0) {
         // ================= issuer =================
+        int ncopy[2] = {}, nused[2] = {}, last_commit = -1;  // for the drain after an abort
         auto map_copy = [&](int c, int st) {
             mbar_expect_tx(full(st), DIG * B_TILE);
             bulk_g2s(smem_u32(sm + S::MAP + st * DIG * B_TILE), a.vdig + ((size_t)m * a.nch + c) * DIG * B_TILE,
                      DIG * B_TILE, full(st));
+            ncopy[st]++;
         };
         const uint32_t idesc_uu = idesc_i8(0, 0, ROWS, COLS), idesc_su = idesc_i8(1, 0, ROWS, COLS),
                        idesc_us = idesc_i8(0, 1, ROWS, COLS), idesc_ss = idesc_i8(1, 1, ROWS, COLS);
@@ -1083,6 +1110,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArg
             if (k >= 1 && !wait(done(gs ^ 1), ((k - 1) >> 1) & 1)) continue;
             if (k + 1 < nck) map_copy(c - 1, gs ^ 1);
             if (!wait(full(gs), (k >> 1) & 1)) continue;
+            nused[gs]++;
             tc_fence_after();
             const uint64_t da0 = smem_desc(smem_u32(sm + S::GEN + gs * DIG * A_TILE), ROWS * 16, 128);
             const uint64_t db0 = smem_desc(smem_u32(sm + S::MAP + gs * DIG * B_TILE), COLS * 16, 128);
@@ -1099,8 +1127,14 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_syn_kernel(SplitSynArg
                     first_lev[lev] = false;
                 }
             mma_commit(done(gs));
+            last_commit = k;
         }
-        wait(done((nck - 1) & 1), ((nck - 1) >> 1) & 1);
+        if (!wait(done((nck - 1) & 1), ((nck - 1) >> 1) & 1)) {
+            // as split_kernel: drain this CTA's copies and MMAs in flight
+            for (int st = 0; st < 2; st++)
+                if (ncopy[st] > nused[st]) drain_wait(full(st), (ncopy[st] - 1) & 1);
+            if (last_commit >= 0) drain_wait(done(last_commit & 1), (last_commit >> 1) & 1);
+        }
     }
     tc_fence_before();
     __syncthreads();

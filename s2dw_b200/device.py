@@ -177,8 +177,14 @@ class Plan:
         check(lib().s2dwc_plan_reserve(self._h, int(nmaps), self._stream(stream)))
 
     def check(self):
-        """Raises S2DWError if a split-form kernel gave up waiting (synchronises)."""
+        """Raises S2DWError if a split-form kernel gave up waiting since the
+        last check (synchronises; the flag is cleared when reported)."""
         check(lib().s2dwc_plan_check(self._h))
+
+    def set_wait_limit(self, ns):
+        """Bound in nanoseconds on every wait of the split-form kernels'
+        pipeline (default 2e9)."""
+        check(lib().s2dwc_plan_set_wait_limit(self._h, int(ns)))
 
     def synthesis(self, wav, scoeff, flm, stream=None):
         import torch

@@ -2,7 +2,7 @@
 large configuration B=2048, N=8, alpha=2, J=Jmax=11, for the GPU parity test
 of the full-band scales (tests/test_gpu_headline_parity.py).
 
-  python tests/golden/make_b2048_fixture.py [threads]
+  python tests/golden/make_b2048_fixture.py [threads] [--add-accurate]
 
 The oracle (oracle/, the CPU restatement of the reference loops) runs
 unsampled on every scale; it takes tens of minutes on 8 cores.  The full
@@ -20,6 +20,15 @@ synthesis of seeded random coefficients (scale by scale, in scale order,
   the rows flm(l, 0:l) for l in SYN_ROWS, and max|flm| over all (l, m).
 
 Tables come from the oracle's init_kernels / init_directionality.
+
+Each output is stored twice: from the oracle as it restates the reference
+(keys ana_rows_j, ana_max_j, syn_row_l, syn_max), and from the oracle with its
+d(pi/2) planes replaced by the accurate long-double planes of
+oracle.dl_plane_accurate (keys with the suffix _acc).  At l ~ 2000 the
+reference's Turok-Bucher planes carry up to 1.4e-13 absolute error (measured
+against 50-digit values), so the second set separates that error from any
+other difference.  --add-accurate computes only the second set and adds it to
+an existing fixture.
 """
 import os
 import sys
@@ -60,34 +69,47 @@ def synthesis_inputs(J, bls, bs):
     return wav, np.asfortranarray(sc)
 
 
-def main():
-    from oracle import oracle as O
+def run(O, K, P, S, J, bls, bs, suffix, out):
     from s2dw_b200.workload import gaussian_flm
 
-    threads = int(sys.argv[1]) if len(sys.argv) > 1 else (os.cpu_count() or 1)
-    O.set_num_threads(threads)
-    J = O.comp_jmax(B, ALPHA)
-    K, P, bs = O.init_kernels(J, B, ALPHA)
-    S = O.init_directionality(B, N)
-    bls = [O.band_limits(j, B, ALPHA)[0] for j in range(J + 1)]
-    out = {"B": B, "N": N, "alpha": ALPHA, "J": J, "power": POWER, "syn_seed": SYN_SEED,
-           "syn_rows": np.array(SYN_ROWS), "bl": np.array(bls)}
     flm = gaussian_flm(B, seed=0, power=POWER)
     t0 = time.time()
     for j in range(J + 1):
         w = O.analysis_scale(j, flm, K, S, J, B, N, ALPHA)
         pairs = rows_for_scale(j, bls[j])
         out[f"ana_pairs_{j}"] = np.array(pairs)
-        out[f"ana_rows_{j}"] = np.stack([w[:, b, g] for b, g in pairs])
-        out[f"ana_max_{j}"] = np.abs(w).max()
-        print(f"analysis scale {j} (bl={bls[j]}): {time.time() - t0:.0f} s", flush=True)
+        out[f"ana_rows_{j}{suffix}"] = np.stack([w[:, b, g] for b, g in pairs])
+        out[f"ana_max_{j}{suffix}"] = np.abs(w).max()
+        print(f"analysis{suffix} scale {j} (bl={bls[j]}): {time.time() - t0:.0f} s", flush=True)
         del w
     wav, sc = synthesis_inputs(J, bls, bs)
     f = O.synthesis_dynamic(wav, sc, K, P, S, J, B, N, bs, ALPHA)
-    print(f"synthesis: {time.time() - t0:.0f} s", flush=True)
+    print(f"synthesis{suffix}: {time.time() - t0:.0f} s", flush=True)
     for l in SYN_ROWS:
-        out[f"syn_row_{l}"] = f[l, :l + 1].copy()
-    out["syn_max"] = np.abs(f).max()
+        out[f"syn_row_{l}{suffix}"] = f[l, :l + 1].copy()
+    out[f"syn_max{suffix}"] = np.abs(f).max()
+
+
+def main():
+    from oracle import oracle as O
+
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    threads = int(args[0]) if args else (os.cpu_count() or 1)
+    O.set_num_threads(threads)
+    J = O.comp_jmax(B, ALPHA)
+    K, P, bs = O.init_kernels(J, B, ALPHA)
+    S = O.init_directionality(B, N)
+    bls = [O.band_limits(j, B, ALPHA)[0] for j in range(J + 1)]
+    if "--add-accurate" in sys.argv:
+        out = dict(np.load(OUT))
+    else:
+        out = {"B": B, "N": N, "alpha": ALPHA, "J": J, "power": POWER, "syn_seed": SYN_SEED,
+               "syn_rows": np.array(SYN_ROWS), "bl": np.array(bls)}
+        O.set_dl_method(0)
+        run(O, K, P, S, J, bls, bs, "", out)
+    O.set_dl_method(1)
+    run(O, K, P, S, J, bls, bs, "_acc", out)
+    O.set_dl_method(0)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT}")
 

@@ -16,6 +16,16 @@ coefficients with max|flm|.
 Tolerance: 1e-12 relative to the scale's max|w| (analysis) or to max|flm|
 (synthesis), the plain FP64 form's parity bar.  The measured errors are
 printed (pytest -s shows them).
+
+At l ~ 2000 the reference's own d(pi/2) planes (Turok-Bucher, restated by the
+oracle) are off by up to 1.4e-13 absolute (tests/test_oracle.py, against
+50-digit values), which moves the reference's full-band coefficients at
+B=2048 by about 1e-12 of max|w|.  The oracle can swap those planes for
+accurate long-double ones (oracle.set_dl_method(1); everything else the
+reference's algorithm), so the tests also compare against that variant: the
+1e-12 bar applies there, and against the plain restatement the difference
+must be the restatement's own plane error (bounded by 2e-12, and at least
+ten times the difference from the accurate variant).
 """
 import os
 import sys
@@ -68,7 +78,17 @@ def test_b1024_every_scale_matches_the_unsampled_oracle():
           " ".join(f"{e:.1e}" for e in errs))
     np.testing.assert_array_equal(sc, sc_ref)
     assert max(errs) <= TOL, errs
-    del wav, ref
+    # the full-band scales against the oracle with accurate d(pi/2) planes
+    O.set_dl_method(1)
+    try:
+        acc = [O.analysis_scale(j, flm, t["K_gamma"], t["Slm"], J, B, N, alpha) for j in (0, 1)]
+    finally:
+        O.set_dl_method(0)
+    eacc = [np.abs(wav[j] - acc[j]).max() / np.abs(acc[j]).max() for j in (0, 1)]
+    print("B=1024 N=4 full-band scales vs the oracle with accurate d(pi/2) planes:",
+          " ".join(f"{e:.1e}" for e in eacc))
+    assert max(eacc) <= TOL
+    del wav, ref, acc
 
     bls = [core.band_limits(j, B, alpha)[0] for j in range(J + 1)]
     rw, rsc = _random_coefficients(np.random.default_rng(1024), bls, N, bs)
@@ -97,12 +117,26 @@ def test_b2048_analysis_rows_match_the_oracle_fixture():
     t = transform_setup(B, N, alpha, J)
     flm = gaussian_flm(B, seed=0, power=float(g["power"]))
     wav, _ = core.s2dw_core_analysis_flm2wav_dynamic(flm, t["K_gamma"], t["Slm"], J, B, N, t["bl_scoeff"], alpha)
-    errs = []
+    errs, eacc, dref = [], [], []
     for j in range(J + 1):
         rows = np.stack([wav[j][:, b, gg] for b, gg in g[f"ana_pairs_{j}"]])
-        errs.append(np.abs(rows - g[f"ana_rows_{j}"]).max() / float(g[f"ana_max_{j}"]))
-    print("\nB=2048 N=8 analysis, sampled rows, max|dw|/max|w| per scale:", " ".join(f"{e:.1e}" for e in errs))
-    assert max(errs) <= TOL, errs
+        mx, mxa = float(g[f"ana_max_{j}"]), float(g[f"ana_max_{j}_acc"])
+        if mxa == 0:  # a scale with an empty l range
+            assert np.abs(rows).max() == 0 and mx == 0, f"scale {j}"
+            errs.append(0.0), eacc.append(0.0), dref.append(0.0)
+            continue
+        errs.append(np.abs(rows - g[f"ana_rows_{j}"]).max() / mx)
+        eacc.append(np.abs(rows - g[f"ana_rows_{j}_acc"]).max() / mxa)
+        dref.append(np.abs(g[f"ana_rows_{j}"] - g[f"ana_rows_{j}_acc"]).max() / mxa)
+    print("\nB=2048 N=8 analysis, sampled rows, max|dw|/max|w| per scale:")
+    print("  GPU vs oracle with accurate d planes:      ", " ".join(f"{e:.1e}" for e in eacc))
+    print("  GPU vs oracle (reference's d planes):      ", " ".join(f"{e:.1e}" for e in errs))
+    print("  oracle: reference's vs accurate d planes:  ", " ".join(f"{e:.1e}" for e in dref))
+    assert max(eacc) <= TOL, eacc
+    assert max(errs) <= 2 * TOL, errs
+    for j in range(J + 1):  # what separates the GPU from the plain restatement is the latter's plane error
+        if errs[j] > TOL / 10:
+            assert eacc[j] <= errs[j] / 10 and dref[j] >= errs[j] / 2, (j, errs[j], eacc[j], dref[j])
 
 
 @pytest.mark.gpu
@@ -118,10 +152,13 @@ def test_b2048_synthesis_rows_match_the_oracle_fixture():
     f = core.s2dw_core_synthesis_wav2flm_dynamic(wav, sc, t["K_gamma"], t["Phi2"], t["Slm"], J, B, N,
                                                  t["bl_scoeff"], alpha)
     del wav
-    worst = {}
+    worst, wacc = {}, {}
     for l in g["syn_rows"]:
         l = int(l)
         worst[l] = np.abs(f[l, :l + 1] - g[f"syn_row_{l}"]).max() / float(g["syn_max"])
-    print("\nB=2048 N=8 synthesis of random coefficients, sampled l-rows, max|df|/max|f|:",
-          " ".join(f"l={k}:{v:.1e}" for k, v in worst.items()))
-    assert max(worst.values()) <= TOL, worst
+        wacc[l] = np.abs(f[l, :l + 1] - g[f"syn_row_{l}_acc"]).max() / float(g["syn_max_acc"])
+    print("\nB=2048 N=8 synthesis of random coefficients, sampled l-rows, max|df|/max|f|:")
+    print("  vs accurate d planes:", " ".join(f"l={k}:{v:.1e}" for k, v in wacc.items()))
+    print("  vs reference's planes:", " ".join(f"l={k}:{v:.1e}" for k, v in worst.items()))
+    assert max(wacc.values()) <= TOL, wacc
+    assert max(worst.values()) <= 2 * TOL, worst

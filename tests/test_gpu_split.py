@@ -86,3 +86,57 @@ def test_split_b256_n5():
     assert worst <= TOL_W, f"max|dw|/max|w| = {worst:.3e}"
     assert syn <= TOL_W, f"max|dflm|/max|flm| = {syn:.3e}"
     assert recon <= TOL_RECON, f"recon {recon:.3e}"
+
+
+@pytest.mark.gpu
+def test_bounded_wait_gives_up_then_the_plan_recovers():
+    """Failure detection without a GPU fault: with a wait limit of 0 every
+    split-kernel wait that is not already satisfied gives up at once; the
+    kernels drain their own copies and tensor-core operations, free their
+    tensor memory and return, and s2dwc_plan_check reports S2DW_ERROR 15
+    (once).  The same plan at the default 2 s limit then gives the FP64
+    results again, and a second check is clean."""
+    import torch
+
+    from s2dw_b200._lib import S2DWError
+    from s2dw_b200.device import Plan
+
+    B, N, alpha, nmaps = 64, 4, 2.0, 3
+    t = transform_setup(B, N, alpha)
+    J = t["J"]
+    plain = Plan(B, N, alpha, J)
+    split = Plan(B, N, alpha, J, form=Plan.SPLIT)
+    for p in (plain, split):
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    flms = [gaussian_flm(B, seed=300 + k) for k in range(nmaps)]
+    d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
+    bs2 = max(1, t["bl_scoeff"] ** 2)
+    w_ref = torch.empty((nmaps, plain.wav_size), dtype=torch.float64, device="cuda")
+    s_ref = torch.empty((nmaps, bs2), dtype=torch.complex128, device="cuda")
+    w_sp = torch.empty_like(w_ref)
+    s_sp = torch.empty_like(s_ref)
+    plain.analysis_batch(d_flm, w_ref, s_ref)
+
+    split.set_wait_limit(0)
+    split.analysis_batch(d_flm, w_sp, s_sp)
+    out = torch.empty_like(d_flm)
+    split.synthesis_batch(w_ref, s_ref, out)
+    with pytest.raises(S2DWError) as e:
+        split.check()
+    assert e.value.code == 15 and "gave up" in str(e.value)
+
+    split.set_wait_limit(2_000_000_000)
+    split.analysis_batch(d_flm, w_sp, s_sp)
+    split.check()
+    torch.cuda.synchronize()
+    wr, ws = w_ref.cpu().numpy(), w_sp.cpu().numpy()
+    offs = plain.wav_offsets
+    for k in range(nmaps):
+        for j in range(J + 1):
+            a, b = wr[k, offs[j]:offs[j + 1]], ws[k, offs[j]:offs[j + 1]]
+            if np.abs(a).max() > 0:
+                assert np.abs(a - b).max() <= TOL_W * np.abs(a).max()
+    with pytest.raises(S2DWError):
+        split.set_wait_limit(-1)
+    plain.close()
+    split.close()

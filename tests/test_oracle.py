@@ -38,6 +38,24 @@ def test_dl_planes_match_high_precision_values():
     assert err_lo < 1e-14, err_lo
 
 
+def test_accurate_dl_planes_match_all_high_precision_values():
+    """The diagnostic long-double planes (oracle.dl_plane_accurate) agree with
+    every 50-digit value up to l = 2047 to the double rounding, where the
+    reference's Turok-Bucher planes are off by up to 1.4e-13."""
+    g = np.load(os.path.join(GOLD, "dl_known.npz"))
+    worst, worst_tb = 0.0, 0.0
+    for l in sorted(set(int(x) for x in g["l"])):
+        sel = g["l"] == l
+        D = O.dl_plane_accurate(l)
+        a, b, d = g["a"][sel], g["b"][sel], g["d"][sel]
+        worst = max(worst, np.abs(D[a + l, b + l] - d).max())
+        if l == 2047:
+            T = O.dl_plane(l)
+            worst_tb = np.abs(T[a + l, b + l] - d).max()
+    assert worst < 1e-16, worst
+    assert worst_tb > 1e-13  # the reference algorithm's error the fixture comparison separates
+
+
 def test_dl_closed_forms_l1_l2():
     s2 = np.sqrt(0.5)
     d1 = O.dl_plane(1)  # d^1(pi/2), rows m' = -1..1, cols m = -1..1
