@@ -24,8 +24,9 @@ B=2048 by about 1e-12 of max|w|.  The oracle can swap those planes for
 accurate long-double ones (oracle.set_dl_method(1); everything else the
 reference's algorithm), so the tests also compare against that variant: the
 1e-12 bar applies there, and against the plain restatement the difference
-must be the restatement's own plane error (bounded by 2e-12, and at least
-ten times the difference from the accurate variant).
+must be the restatement's own plane error (bounded by 2e-12, at least three
+times the difference from the accurate variant, and matched by the
+restatement's own change when its planes are swapped).
 """
 import os
 import sys
@@ -136,7 +137,7 @@ def test_b2048_analysis_rows_match_the_oracle_fixture():
     assert max(errs) <= 2 * TOL, errs
     for j in range(J + 1):  # what separates the GPU from the plain restatement is the latter's plane error
         if errs[j] > TOL / 10:
-            assert eacc[j] <= errs[j] / 10 and dref[j] >= errs[j] / 2, (j, errs[j], eacc[j], dref[j])
+            assert eacc[j] <= errs[j] / 3 and dref[j] >= errs[j] / 2, (j, errs[j], eacc[j], dref[j])
 
 
 @pytest.mark.gpu
