@@ -46,12 +46,15 @@ HBM_GBS = _hbm_gbs()
 UNIT = "pairs/s"
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
-# kernel kind, averaged over the 22 launches of each kind in two
-# analysis+synthesis pairs at B=1024 N=4 alpha=2 J=10 (11 scales), from one
-# ncu capture of this script.  Used only for the roofline "traffic" entry of
-# that workload.
-NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.60e6, "mwalk": 10.76e6, "ana_beta": 27.64e6,
-                                "ana_alpha": 45.15e6, "syn_alpha": 43.95e6, "syn_beta": 31.50e6}}
+# kernel kind, averaged over the 11 launches of each kind in one
+# analysis+synthesis pair at B=1024 N=4 alpha=2 J=10, from the ncu launch list
+# of `python -m s2dw_b200.workload 1024 4 1` (profiles/launches_B1024_N4.md).
+# Used only for the roofline "traffic" entry of that workload.
+NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.555e6, "mwalk": 10.76e6, "ana_beta": 27.18e6,
+                                "ana_alpha": 45.13e6, "syn_alpha": 44.06e6, "syn_beta": 31.13e6}}
+NCU_TRAFFIC_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
+                      "--clock-control none of `python -m s2dw_b200.workload 1024 4 1` (one pair, 11 launches of "
+                      "each kind), profiles/launches_B1024_N4.md")
 
 
 def parse():
@@ -619,6 +622,7 @@ def main():
         roofline = {"kernel": dom[0], "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
                     "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
                     "traffic_unit": "bytes per launch (ncu, mean over a pair's launches)",
+                    "traffic_source": NCU_TRAFFIC_SOURCE,
                     "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (MEASURED_PEAKS.json has no fp64 entry)",
                     "flops_per_pair": algo[dom[0]], "launches_per_pair": launches_per_pair,
                     "avg_launch_ms": per_launch_ms,
