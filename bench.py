@@ -213,12 +213,18 @@ def serving_stats(n_requests, device, split_requests=1024):
     from s2dw_b200.serving import Server, make_stream
 
     reqs, inputs = make_stream(n_requests, seed=2026, rate_hz=1e9)
-    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device)
+    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device, priorities=True)
     st = _serve(srv, reqs)
     srv.close()
     st.update({"form": "fp64",
                "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
-                         "half analysis / half synthesis, device-resident inputs, graph replay"})
+                         "half analysis / half synthesis, device-resident inputs, graph replay, slot stream "
+                         "priorities by B (smaller first)"})
+    # the same stream and offered rate with every slot at the default priority (first come, first served)
+    srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device, priorities=False)
+    fifo = _serve(srv, reqs, rate=st["offered_rate_rps"])
+    srv.close()
+    st["fifo"] = {k: fifo[k] for k in ("p50_ms", "p99_ms", "mean_ms", "throughput_rps", "saturation_rps")}
     if split_requests > 0:
         try:
             sub = reqs[:split_requests]

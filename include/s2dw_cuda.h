@@ -256,6 +256,15 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
  * as a status instead of a halt. */
 int s2dwc_plan_check(s2dwc_plan *plan);
 
+/* CUDA stream priority of the plan's per-scale streams (CUDA's convention:
+ * lower values run first; clamped to cudaDeviceGetStreamPriorityRange).  The
+ * plan's kernels, and those of CUDA graphs captured from its calls after
+ * this one, then take SMs ahead of work of lower priority: a server gives
+ * its small, latency-bound transforms precedence over the full-band scales
+ * of large ones.  Waits for the plan's streams to drain; call it between
+ * transforms, outside stream capture.  No counterpart in the reference. */
+int s2dwc_plan_set_priority(s2dwc_plan *plan, int priority);
+
 /* Bound, in nanoseconds, on every wait of the split-form kernels' pipeline
  * (default 2 s).  A kernel whose wait runs out stops its work, lets its own
  * copies and tensor-core operations in flight finish, frees its tensor

@@ -1661,6 +1661,25 @@ int s2dwc_plan_check(s2dwc_plan *p)
     S2DW_API_CATCH
 }
 
+int s2dwc_plan_set_priority(s2dwc_plan *p, int priority)
+{
+    S2DW_API_TRY
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_set_priority: null plan");
+    std::lock_guard<std::mutex> g(p->mu);
+    DeviceGuard dg(p->device);
+    int least = 0, greatest = 0;
+    S2DW_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int prio = std::min(least, std::max(greatest, priority));
+    for (auto &st : p->streams) {
+        S2DW_CUDA_TRY(cudaStreamSynchronize(st));
+        S2DW_CUDA_TRY(cudaStreamDestroy(st));
+        st = nullptr;
+        S2DW_CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio));
+    }
+    return S2DWC_OK;
+    S2DW_API_CATCH
+}
+
 int s2dwc_plan_set_wait_limit(s2dwc_plan *p, long long ns)
 {
     S2DW_API_TRY

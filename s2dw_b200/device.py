@@ -181,6 +181,11 @@ class Plan:
         last check (synchronises; the flag is cleared when reported)."""
         check(lib().s2dwc_plan_check(self._h))
 
+    def set_priority(self, priority):
+        """CUDA stream priority of the plan's per-scale streams (lower runs
+        first); graphs captured afterwards keep it."""
+        check(lib().s2dwc_plan_set_priority(self._h, int(priority)))
+
     def set_wait_limit(self, ns):
         """Bound in nanoseconds on every wait of the split-form kernels'
         pipeline (default 2e9)."""

@@ -61,8 +61,15 @@ def split_batch_capacity(B, N, alpha, J, max_batch=32, batch_bytes=2 << 30):
     return max(1, min(max_batch, int(batch_bytes) // (8 * _wav_size(B, N, alpha, J))))
 
 
+def size_priority(B):
+    """CUDA stream priority of a slot by band limit (lower runs first): the
+    small transforms, a few microseconds of latency-bound kernels each, take
+    SMs ahead of the full-band scales of large ones (shortest job first)."""
+    return 0 if B >= 1024 else -1 if B >= 512 else -2 if B >= 256 else -3
+
+
 class Slot:
-    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=2 << 30):
+    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=2 << 30, priority=None):
         import torch
 
         B, N, alpha, J = key
@@ -72,7 +79,11 @@ class Slot:
         self.plan = Plan(B, N, alpha, J, device=device, form=Plan.SPLIT if self.split else Plan.FP64)
         self.plan.set_tables(tables["K_gamma"], tables["Phi2"], tables["Slm"], tables["bl_scoeff"])
         bs = tables["bl_scoeff"]
-        self.stream = torch.cuda.Stream(device=device)
+        if priority is not None:
+            self.plan.set_priority(priority)
+            self.stream = torch.cuda.Stream(device=device, priority=priority)
+        else:
+            self.stream = torch.cuda.Stream(device=device)
         c = self.cap
         self.d_wav = torch.empty((c, self.plan.wav_size), dtype=torch.float64, device=device)
         self.d_sc = torch.empty((c, max(1, bs * bs)), dtype=torch.complex128, device=device)
@@ -148,10 +159,12 @@ class Slot:
 
 class Server:
     def __init__(self, hbm_budget_bytes=40 << 30, max_inflight=64, slots_per_config=2, use_graphs=True,
-                 device=0, keep_outputs=False, form="fp64", max_batch=32, batch_bytes=2 << 30):
+                 device=0, keep_outputs=False, form="fp64", max_batch=32, batch_bytes=2 << 30,
+                 priorities=False):
         if form not in ("fp64", "split"):
             raise ValueError(f"form must be 'fp64' or 'split', not {form!r}")
         self.form = form
+        self.priorities = priorities  # slots' stream priorities by size (size_priority)
         self.max_batch = max_batch
         self.batch_bytes = batch_bytes
         self.budget = int(hbm_budget_bytes)
@@ -192,7 +205,8 @@ class Server:
         while self.used + est > self.budget:
             if not self._evict_one(key):
                 return None
-        s = Slot(key, self.config_tables(B, N, alpha, J), self.device, self.form, self.max_batch, self.batch_bytes)
+        s = Slot(key, self.config_tables(B, N, alpha, J), self.device, self.form, self.max_batch, self.batch_bytes,
+                 priority=size_priority(B) if self.priorities else None)
         self.slots[key].append(s)
         self.used += s.bytes
         return s

@@ -6,14 +6,16 @@ import pytest
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("use_graphs", [True, False])
-def test_results_identical_alone_and_in_mix(use_graphs):
+@pytest.mark.parametrize("use_graphs,priorities", [(True, False), (False, False), (True, True)])
+def test_results_identical_alone_and_in_mix(use_graphs, priorities):
     from s2dw_b200.serving import Server, make_stream
 
-    reqs, inputs = make_stream(40, seed=3, rate_hz=20000.0, Bs=(32, 48, 64, 128), Ns=range(1, 9),
+    reqs, inputs = make_stream(40, seed=3, rate_hz=20000.0, Bs=(32, 48, 64, 128, 256, 512), Ns=range(1, 9),
                                alphas=(2.0, 3.0), pool=2)
     # in the mix: everything arrives within ~2 ms, many requests overlap
-    srv = Server(hbm_budget_bytes=8 << 30, slots_per_config=2, use_graphs=use_graphs, keep_outputs=True)
+    # (with priorities, the small requests' kernels overtake the larger ones')
+    srv = Server(hbm_budget_bytes=8 << 30, slots_per_config=2, use_graphs=use_graphs, keep_outputs=True,
+                 priorities=priorities)
     stats = srv.run(reqs)
     srv.close()
     assert stats["requests"] == len(reqs)

@@ -12,8 +12,9 @@ from s2dw_b200 import serving
 class _StubSlot:
     closed = []
 
-    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=0):
+    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=0, priority=None):
         self.key = key
+        self.priority = priority
         self.bytes = _StubSlot.estimate_bytes(*key, form, max_batch, batch_bytes)
         self.busy = False
         self.last_used = 0.0
@@ -70,3 +71,18 @@ def test_lru_eviction_of_idle_slots_of_other_configs(srv):
     b2 = srv._acquire(Bk, 4.0)                     # evicts a1; b1 is busy, and B's own slots are kept
     assert b2 is not None and _StubSlot.closed == [A, A] and srv.used == 2000
     assert srv.used <= srv.budget
+
+
+def test_size_priority_orders_small_transforms_first(monkeypatch):
+    """With priorities on, a slot's stream priority follows its band limit:
+    smaller transforms get numerically lower (higher) CUDA priorities."""
+    prios = [serving.size_priority(B) for B in (32, 64, 128, 256, 512, 1024, 2048)]
+    assert prios == sorted(prios) and prios[0] < prios[-1] == 0
+    monkeypatch.setattr(serving, "Slot", _StubSlot)
+    s = serving.Server(hbm_budget_bytes=1 << 20, priorities=True)
+    monkeypatch.setattr(s, "config_tables", lambda *k: None)
+    small, big = s._acquire((64, 2, 2.0, 6), 0.0), s._acquire((1024, 2, 2.0, 10), 0.0)
+    assert small.priority < big.priority == 0
+    s2 = serving.Server(hbm_budget_bytes=1 << 20)
+    monkeypatch.setattr(s2, "config_tables", lambda *k: None)
+    assert s2._acquire((64, 2, 2.0, 6), 0.0).priority is None
