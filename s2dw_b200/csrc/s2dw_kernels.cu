@@ -481,26 +481,40 @@ __device__ __forceinline__ void mwalk_body(const MwalkArgs &a)
         }
         const double2 *Vb = reinterpret_cast<const double2 *>(b + L::V_OFF);
         const bool ramp = (c0 + MW_CH - 1 >= lbase);
+        // one step of the m' walk for pair q at chunk row k (the same
+        // operations in the same order on both paths below)
+        auto mstep = [&](const int k, const int q) {
+            double zr = 0.0, zi = 0.0;
 #pragma unroll
-        for (int k = MW_CH - 1; k >= 0; k--) {
-            const int mpv = c0 + k;
-            if (mpv > MH) continue;  // above the top of this tile (warp-uniform)
+            for (int kq = 0; kq < NP; kq++) {
+                const double2 v = Vb[(kq * WQ + w * Q + q) * MW_CH + k];
+                zr = fma(gr[kq][k], v.x, zr);
+                zi = fma(gr[kq][k], v.y, zi);
+            }
+            acc[q].x = fma(e[q], zr, acc[q].x);
+            acc[q].y = fma(e[q], zi, acc[q].y);
+            const double p = mq[q] * br[k];
+            const double en = fma(p, e[q], -ep[q]);
+            ep[q] = e[q];
+            e[q] = en;
+        };
+        if (!ramp && c0 + MW_CH - 1 <= MH) {
+            // a chunk below the tile's l rows: every step runs, no start value
+            // enters (warp-uniform)
 #pragma unroll
-            for (int q = 0; q < Q; q++) {
-                if (ramp && mpv == l) e[q] = st[q];
-                double zr = 0.0, zi = 0.0;
+            for (int k = MW_CH - 1; k >= 0; k--)
 #pragma unroll
-                for (int kq = 0; kq < NP; kq++) {
-                    const double2 v = Vb[(kq * WQ + w * Q + q) * MW_CH + k];
-                    zr = fma(gr[kq][k], v.x, zr);
-                    zi = fma(gr[kq][k], v.y, zi);
+                for (int q = 0; q < Q; q++) mstep(k, q);
+        } else {
+#pragma unroll
+            for (int k = MW_CH - 1; k >= 0; k--) {
+                const int mpv = c0 + k;
+                if (mpv > MH) continue;  // above the top of this tile (warp-uniform)
+#pragma unroll
+                for (int q = 0; q < Q; q++) {
+                    if (ramp && mpv == l) e[q] = st[q];
+                    mstep(k, q);
                 }
-                acc[q].x = fma(e[q], zr, acc[q].x);
-                acc[q].y = fma(e[q], zi, acc[q].y);
-                const double p = mq[q] * br[k];
-                const double en = fma(p, e[q], -ep[q]);
-                ep[q] = e[q];
-                e[q] = en;
             }
         }
         if (Kw > 0) {
@@ -1206,8 +1220,27 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 
     __syncthreads();
 
     double2 v[16];
+    if (MODE == FFT_SYN_BETA) {
+        // gamma DFT of the row with coalesced loads (b contiguous across the
+        // threads), then the DCT-II reordering through shared memory: the
+        // value of b goes to FFT index b/2 (b even) or (4bl-1-b)/2 (b odd)
+        const bool sn = (rr + a.nq[g]) & 1;
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
+        for (int i = 0; i < 16; i++) {
+            const int b = t + i * THREADS;
+            double2 u = zero;
+            for (int gg = 0; gg < N; gg++) u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + b], ph[gg]));
+            u = cscale(u, a.wq[b]);
+            if (sn && (b & 1)) u = make_double2(-u.x, -u.y);
+            buf[padix((b & 1) ? (4 * bl - 1 - b) >> 1 : b >> 1)] = u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = buf[padix(lpos<LGM, R0>(t, i))];
+        __syncthreads();  // the exchanges of the FFT reuse buf
+    }
+#pragma unroll
+    for (int i = 0; i < 16 && MODE != FFT_SYN_BETA; i++) {
         const int k = lpos<LGM, R0>(t, i);
         double2 x = zero;
         if (MODE == CZT_ANA_ALPHA) {  // (g, b pair rr); Hermitian completion in m
@@ -1234,12 +1267,6 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 
             }
         } else if (MODE == FFT_ANA_BETA) {  // (g, m = rr), DCT-III input
             x = ana_beta_in(a.in_c + ((size_t)g * bl + rr) * bl, k, bl, (rr + N - 1) & 1, a.czt.pre);
-        } else if (MODE == FFT_SYN_BETA) {  // (q = g, m = rr), DCT-II input at b = beta_src(k)
-            const int b = beta_src(k, bl);
-            double2 u = zero;
-            for (int gg = 0; gg < N; gg++) u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + b], ph[gg]));
-            x = cscale(u, a.wq[b]);
-            if (((rr + a.nq[g]) & 1) && (b & 1)) x = make_double2(-x.x, -x.y);
         } else {  // CZT_SYN_BETA, (q = g, m = rr), k = b
             if (k < 2 * bl) {
                 double2 u = zero;
