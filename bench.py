@@ -215,7 +215,12 @@ def serving_stats(n_requests, device, split_requests=1024):
     reqs, inputs = make_stream(n_requests, seed=2026, rate_hz=1e9)
     srv = Server(hbm_budget_bytes=60 << 30, slots_per_config=2, use_graphs=True, device=device, priorities=True)
     st = _serve(srv, reqs)
+    # the stream's device time with the requests run one at a time: the
+    # saturation span against it is the overlap the server achieves
+    serial = srv.device_time(reqs)
     srv.close()
+    st["serial_device_s"] = serial
+    st["overlap_vs_serial"] = serial * st["saturation_rps"] / len(reqs)
     st.update({"form": "fp64",
                "stream": f"{n_requests} requests, Poisson, B in 32..1024, N in 1..8, alpha in {{2,3}}, J=Jmax, "
                          "half analysis / half synthesis, device-resident inputs, graph replay, slot stream "
@@ -803,6 +808,7 @@ def main():
             "split_max_w_err": g(split, "max_w_err"), "split_b256_vs_fp64": g(split_b256, "speedup_vs_fp64"),
             "large_b2048_pairs_s": g(large, "value"), "large_split_vs_fp64": g(large, "split", "speedup_vs_fp64"),
             "serving_saturation_rps": g(serving, "saturation_rps"),
+            "serving_serial_device_s": g(serving, "serial_device_s"),
             "serving_rps": g(serving, "throughput_rps"), "serving_p50_ms": g(serving, "p50_ms"),
             "serving_p99_ms": g(serving, "p99_ms"), "serving_split_p50_ms": g(serving, "split", "p50_ms"),
             "serving_split_p99_ms": g(serving, "split", "p99_ms"),

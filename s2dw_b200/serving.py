@@ -100,6 +100,9 @@ class Slot:
         self.graphs = {}
         self.busy = False
         self.last_used = 0.0
+        # recorded just before the slot's last batch starts (its device time
+        # when the batch runs alone: Server.device_time)
+        self.ev_start = torch.cuda.Event(enable_timing=True)
 
     def run(self, reqs, use_graphs):
         """Enqueue the transform of a batch of requests (one request in the
@@ -141,8 +144,10 @@ class Slot:
                     with torch.cuda.graph(g, stream=self.stream):
                         body()
                     self.graphs[gkey] = g
+                self.ev_start.record(self.stream)
                 g.replay()
             else:
+                self.ev_start.record(self.stream)
                 body()
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(self.stream)
@@ -292,6 +297,23 @@ class Server:
                 "throughput_rps": len(done) / span, "wall_s": t_end, "form": self.form,
                 "batches": len(batches), "mean_batch": float(np.mean(batches)) if batches else 0.0,
                 "slots": sum(len(v) for v in self.slots.values()), "hbm_bytes": self.used}
+
+    def device_time(self, requests):
+        """Sum over `requests` of each one's device time run alone (one at a
+        time, graphs and slots already warm): the stream's GPU work with no
+        overlap between requests, against which a saturation span shows how
+        much the server overlaps requests and whether the host loop limits it."""
+        import torch
+
+        torch.cuda.set_device(self.device)
+        total = 0.0
+        for r in requests:
+            key = (r.B, r.N, r.alpha, r.J)
+            s = self._acquire(key, 0.0)
+            ev = s.run([r], self.use_graphs)
+            ev.synchronize()
+            total += s.ev_start.elapsed_time(ev) / 1e3
+        return total
 
     def close(self):
         for lst in self.slots.values():
