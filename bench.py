@@ -234,17 +234,43 @@ def serving_stats(n_requests, device, split_requests=1024):
         try:
             sub = reqs[:split_requests]
             srv = Server(hbm_budget_bytes=80 << 30, slots_per_config=2, use_graphs=True, device=device,
-                         form="split", batch_bytes=1 << 30)
+                         form="split", batch_bytes=1 << 30, split_min_batch=16)
             sp = _serve(srv, sub, rate=st["offered_rate_rps"])
             srv.close()
             sp["note"] = (f"split-precision slots: waiting requests of one configuration and kind run as one "
-                          f"tensor-core batch; the first {len(sub)} requests of the FP64 server's stream at its "
-                          f"offered rate")
+                          f"tensor-core batch, batches under 16 maps in FP64; the first {len(sub)} requests of "
+                          f"the FP64 server's stream at its offered rate")
             st["split"] = sp
         except Exception as ex:  # reported, not fatal to the bench line
             st["split"] = {"error": str(ex)[:300]}
+        try:
+            st["burst"] = burst_stats(device)
+        except Exception as ex:
+            st["burst"] = {"error": str(ex)[:300]}
     del inputs
     return st
+
+
+def burst_stats(device, n=512):
+    """A burst of one configuration (B=1024, N=4, alpha=2, half analyses and
+    half syntheses, all arriving at once), served by the FP64 server and by
+    the split server (batches of up to 32 maps of one configuration and kind;
+    under 16 maps in FP64): where the split form pays in serving."""
+    from s2dw_b200.serving import Server, make_stream
+
+    reqs, inputs = make_stream(n, seed=11, rate_hz=1e9, Bs=(1024,), Ns=(4,), alphas=(2.0,))
+    out = {"stream": f"{n} requests of B=1024 N=4 alpha=2 J=10, half analysis / half synthesis, all at once"}
+    for name, kw in (("fp64", {}), ("split", {"form": "split", "batch_bytes": 12 << 30, "split_min_batch": 16})):
+        srv = Server(hbm_budget_bytes=80 << 30, slots_per_config=2, use_graphs=True, device=device, **kw)
+        for r in reqs:
+            r.arrival = 0.0
+        srv.run(reqs)  # warm-up: slots and graphs of every batch size met
+        st = srv.run(reqs)
+        srv.close()
+        out[name] = {k: st[k] for k in ("throughput_rps", "p50_ms", "p99_ms", "mean_batch")}
+    out["split_vs_fp64"] = out["split"]["throughput_rps"] / out["fp64"]["throughput_rps"]
+    del inputs
+    return out
 
 
 def split_stats(B, N, alpha, J, maps, repeats=3, power=1.0):
@@ -812,6 +838,7 @@ def main():
             "serving_rps": g(serving, "throughput_rps"), "serving_p50_ms": g(serving, "p50_ms"),
             "serving_p99_ms": g(serving, "p99_ms"), "serving_split_p50_ms": g(serving, "split", "p50_ms"),
             "serving_split_p99_ms": g(serving, "split", "p99_ms"),
+            "serving_burst_split_vs_fp64": g(serving, "burst", "split_vs_fp64"),
         }
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -256,6 +256,15 @@ int s2dwc_stat_moments(double *const *wav_scales, int J, int B, int N, double al
  * as a status instead of a halt. */
 int s2dwc_plan_check(s2dwc_plan *plan);
 
+/* Split-form plans: batches of fewer than `nmaps` maps run the FP64 path
+ * (default 1: every batch runs the split contractions).  The split form
+ * generates the Wigner-d digits once per batch, so it pays only from a
+ * batch size on (about 17 maps at B=1024, N=4); a server that meets
+ * batches of every size sets it to that crossover.  The results of a map
+ * then depend on its batch's size, within the split form's 1e-10 bound.
+ * No counterpart in the reference. */
+int s2dwc_plan_set_split_min_batch(s2dwc_plan *plan, int nmaps);
+
 /* CUDA stream priority of the plan's per-scale streams (CUDA's convention:
  * lower values run first; clamped to cudaDeviceGetStreamPriorityRange).  The
  * plan's kernels, and those of CUDA graphs captured from its calls after

@@ -48,6 +48,7 @@ SIGNATURES = {
     "s2dwc_plan_check": (_i, [_vp]),
     "s2dwc_plan_set_wait_limit": (_i, [_vp, ctypes.c_longlong]),
     "s2dwc_plan_set_priority": (_i, [_vp, _i]),
+    "s2dwc_plan_set_split_min_batch": (_i, [_vp, _i]),
     "s2dwc_plan_reserve": (_i, [_vp, _i, _vp]),
     "s2dwc_plan_stat_moments": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "s2dwc_stat_moments": (_i, [ctypes.POINTER(_dp), _i, _i, _i, _d, _dp, _dp, _dp, _dp, ctypes.POINTER(_dp),

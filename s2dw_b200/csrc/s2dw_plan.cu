@@ -117,6 +117,7 @@ struct s2dwc_plan {
     long long sp_tg_map = 0, sp_v2f_map = 0;
     int *sp_err = nullptr;
     unsigned long long sp_wait_ns = 2000000000ull;  // bound on every split-kernel pipeline wait (2 s)
+    int sp_min_batch = 1;  // split-form batches smaller than this run the FP64 path
     // moments of the coefficients (built on first use): 32 maps per pass
     double *st_part = nullptr, *st_mean = nullptr;
     int *st_flags = nullptr;
@@ -1481,7 +1482,7 @@ int s2dwc_plan_analysis_batch(s2dwc_plan *p, int nmaps, double *d_wav, double *d
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_analysis_batch: tables not set");
     DeviceGuard dg(p->device);
     cudaStream_t s = (cudaStream_t)stream;
-    if (p->form == S2DWC_FORM_SPLIT)
+    if (p->form == S2DWC_FORM_SPLIT && nmaps >= p->sp_min_batch)
         return run_analysis_split(p, nmaps, d_wav, reinterpret_cast<double2 *>(d_scoeff),
                                   reinterpret_cast<const double2 *>(d_flm), s);
     const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
@@ -1504,7 +1505,7 @@ int s2dwc_plan_synthesis_batch(s2dwc_plan *p, int nmaps, double *d_flm, const do
     if (nmaps < 0) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_synthesis_batch: nmaps=%d", nmaps);
     if (!p->tables_set) return set_error(S2DWC_ERROR_NOT_INIT, "plan_synthesis_batch: tables not set");
     DeviceGuard dg(p->device);
-    if (p->form == S2DWC_FORM_SPLIT)
+    if (p->form == S2DWC_FORM_SPLIT && nmaps >= p->sp_min_batch)
         return run_synthesis_split(p, nmaps, reinterpret_cast<double2 *>(d_flm), d_wav,
                                    reinterpret_cast<const double2 *>(d_scoeff), (cudaStream_t)stream);
     const long long wtot = p->wav_off[p->J + 1], B2 = (long long)p->B * p->B;
@@ -1676,6 +1677,16 @@ int s2dwc_plan_set_priority(s2dwc_plan *p, int priority)
         st = nullptr;
         S2DW_CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio));
     }
+    return S2DWC_OK;
+    S2DW_API_CATCH
+}
+
+int s2dwc_plan_set_split_min_batch(s2dwc_plan *p, int nmaps)
+{
+    S2DW_API_TRY
+    if (!p) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_set_split_min_batch: null plan");
+    if (nmaps < 1) return set_error(S2DWC_ERROR_ARG_INVALID, "plan_set_split_min_batch: nmaps=%d", nmaps);
+    p->sp_min_batch = nmaps;
     return S2DWC_OK;
     S2DW_API_CATCH
 }

@@ -181,6 +181,11 @@ class Plan:
         last check (synchronises; the flag is cleared when reported)."""
         check(lib().s2dwc_plan_check(self._h))
 
+    def set_split_min_batch(self, nmaps):
+        """Split-form plans: batches of fewer than `nmaps` maps run the FP64
+        path (default 1)."""
+        check(lib().s2dwc_plan_set_split_min_batch(self._h, int(nmaps)))
+
     def set_priority(self, priority):
         """CUDA stream priority of the plan's per-scale streams (lower runs
         first); graphs captured afterwards keep it."""

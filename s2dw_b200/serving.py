@@ -69,7 +69,8 @@ def size_priority(B):
 
 
 class Slot:
-    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=2 << 30, priority=None):
+    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=2 << 30, priority=None,
+                 split_min_batch=1):
         import torch
 
         B, N, alpha, J = key
@@ -78,6 +79,8 @@ class Slot:
         self.cap = split_batch_capacity(B, N, alpha, J, max_batch, batch_bytes) if self.split else 1
         self.plan = Plan(B, N, alpha, J, device=device, form=Plan.SPLIT if self.split else Plan.FP64)
         self.plan.set_tables(tables["K_gamma"], tables["Phi2"], tables["Slm"], tables["bl_scoeff"])
+        if self.split and split_min_batch > 1:
+            self.plan.set_split_min_batch(split_min_batch)
         bs = tables["bl_scoeff"]
         if priority is not None:
             self.plan.set_priority(priority)
@@ -165,10 +168,13 @@ class Slot:
 class Server:
     def __init__(self, hbm_budget_bytes=40 << 30, max_inflight=64, slots_per_config=2, use_graphs=True,
                  device=0, keep_outputs=False, form="fp64", max_batch=32, batch_bytes=2 << 30,
-                 priorities=False):
+                 priorities=False, split_min_batch=1):
         if form not in ("fp64", "split"):
             raise ValueError(f"form must be 'fp64' or 'split', not {form!r}")
         self.form = form
+        # split slots: batches smaller than this run the FP64 path (the split
+        # form pays from ~17 maps of one configuration at B=1024, N=4)
+        self.split_min_batch = split_min_batch
         self.priorities = priorities  # slots' stream priorities by size (size_priority)
         self.max_batch = max_batch
         self.batch_bytes = batch_bytes
@@ -211,7 +217,7 @@ class Server:
             if not self._evict_one(key):
                 return None
         s = Slot(key, self.config_tables(B, N, alpha, J), self.device, self.form, self.max_batch, self.batch_bytes,
-                 priority=size_priority(B) if self.priorities else None)
+                 priority=size_priority(B) if self.priorities else None, split_min_batch=self.split_min_batch)
         self.slots[key].append(s)
         self.used += s.bytes
         return s

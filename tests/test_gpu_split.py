@@ -140,3 +140,47 @@ def test_bounded_wait_gives_up_then_the_plan_recovers():
         split.set_wait_limit(-1)
     plain.close()
     split.close()
+
+
+@pytest.mark.gpu
+def test_split_min_batch_runs_small_batches_in_fp64():
+    """s2dwc_plan_set_split_min_batch: a split-form plan runs batches under
+    the threshold on the FP64 path (bit-identical to an FP64 plan) and larger
+    ones on the tensor cores (within the split bound)."""
+    import torch
+
+    from s2dw_b200.device import Plan
+
+    B, N, alpha = 64, 4, 2.0
+    t = transform_setup(B, N, alpha)
+    J = t["J"]
+    plain = Plan(B, N, alpha, J)
+    split = Plan(B, N, alpha, J, form=Plan.SPLIT)
+    for p in (plain, split):
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+    split.set_split_min_batch(4)
+    bs2 = max(1, t["bl_scoeff"] ** 2)
+    for nmaps, same in ((2, True), (5, False)):
+        flms = [gaussian_flm(B, seed=500 + k) for k in range(nmaps)]
+        d_flm = torch.from_numpy(np.stack([np.ascontiguousarray(f.T) for f in flms])).cuda()
+        w_ref = torch.empty((nmaps, plain.wav_size), dtype=torch.float64, device="cuda")
+        s_ref = torch.empty((nmaps, bs2), dtype=torch.complex128, device="cuda")
+        w_sp, s_sp = torch.empty_like(w_ref), torch.empty_like(s_ref)
+        plain.analysis_batch(d_flm, w_ref, s_ref)
+        split.analysis_batch(d_flm, w_sp, s_sp)
+        f_ref, f_sp = torch.empty_like(d_flm), torch.empty_like(d_flm)
+        plain.synthesis_batch(w_ref, s_ref, f_ref)
+        split.synthesis_batch(w_ref, s_ref, f_sp)
+        split.check()
+        torch.cuda.synchronize()
+        a, b = w_ref.cpu().numpy(), w_sp.cpu().numpy()
+        fa, fb = f_ref.cpu().numpy(), f_sp.cpu().numpy()
+        if same:
+            np.testing.assert_array_equal(a, b)
+            np.testing.assert_array_equal(fa, fb)
+        else:
+            assert not np.array_equal(a, b)
+            assert np.abs(a - b).max() <= TOL_W * np.abs(a).max()
+            assert np.abs(fa - fb).max() <= TOL_W * np.abs(fa).max()
+    plain.close()
+    split.close()

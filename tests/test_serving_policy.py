@@ -12,7 +12,8 @@ from s2dw_b200 import serving
 class _StubSlot:
     closed = []
 
-    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=0, priority=None):
+    def __init__(self, key, tables, device, form="fp64", max_batch=32, batch_bytes=0, priority=None,
+                 split_min_batch=1):
         self.key = key
         self.priority = priority
         self.bytes = _StubSlot.estimate_bytes(*key, form, max_batch, batch_bytes)
