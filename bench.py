@@ -234,12 +234,13 @@ def serving_stats(n_requests, device, split_requests=1024):
         try:
             sub = reqs[:split_requests]
             srv = Server(hbm_budget_bytes=80 << 30, slots_per_config=2, use_graphs=True, device=device,
-                         form="split", batch_bytes=1 << 30, split_min_batch=16)
+                         form="auto", batch_bytes=12 << 30, split_min_batch=16, priorities=True)
             sp = _serve(srv, sub, rate=st["offered_rate_rps"])
             srv.close()
-            sp["note"] = (f"split-precision slots: waiting requests of one configuration and kind run as one "
-                          f"tensor-core batch, batches under 16 maps in FP64; the first {len(sub)} requests of "
-                          f"the FP64 server's stream at its offered rate")
+            sp["note"] = (f"form auto: split-precision slots (waiting requests of one configuration and kind as "
+                          f"one tensor-core batch of up to 32 maps) where 16 or more of one configuration and kind "
+                          f"wait, FP64 slots otherwise; the first {len(sub)} requests of the FP64 server's stream "
+                          f"at its offered rate")
             st["split"] = sp
         except Exception as ex:  # reported, not fatal to the bench line
             st["split"] = {"error": str(ex)[:300]}
@@ -260,7 +261,7 @@ def burst_stats(device, n=512):
 
     reqs, inputs = make_stream(n, seed=11, rate_hz=1e9, Bs=(1024,), Ns=(4,), alphas=(2.0,))
     out = {"stream": f"{n} requests of B=1024 N=4 alpha=2 J=10, half analysis / half synthesis, all at once"}
-    for name, kw in (("fp64", {}), ("split", {"form": "split", "batch_bytes": 12 << 30, "split_min_batch": 16})):
+    for name, kw in (("fp64", {}), ("split", {"form": "auto", "batch_bytes": 12 << 30, "split_min_batch": 16})):
         srv = Server(hbm_budget_bytes=80 << 30, slots_per_config=2, use_graphs=True, device=device, **kw)
         for r in reqs:
             r.arrival = 0.0

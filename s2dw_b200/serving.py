@@ -17,6 +17,10 @@ tensor-core pass shares the Wigner-d digits among up to 32 maps: a free slot
 takes every waiting request of its configuration and kind (up to the slot's
 batch capacity) as one batch.  The batch's inputs are copied into the slot's
 staging buffers, so one CUDA graph per (kind, batch size) serves every batch.
+With ``form="auto"`` a request goes to a split slot when at least
+``split_min_batch`` requests of its configuration and kind are waiting (the
+batch size from which the split form is faster, about 17 maps at B=1024,
+N=4), and to an FP64 slot otherwise.
 
 Results are identical alone and in a mix: the kernels are deterministic (no
 atomics; the synthesis sums scales in a fixed order), a slot's buffers are
@@ -169,8 +173,8 @@ class Server:
     def __init__(self, hbm_budget_bytes=40 << 30, max_inflight=64, slots_per_config=2, use_graphs=True,
                  device=0, keep_outputs=False, form="fp64", max_batch=32, batch_bytes=2 << 30,
                  priorities=False, split_min_batch=1):
-        if form not in ("fp64", "split"):
-            raise ValueError(f"form must be 'fp64' or 'split', not {form!r}")
+        if form not in ("fp64", "split", "auto"):
+            raise ValueError(f"form must be 'fp64', 'split' or 'auto', not {form!r}")
         self.form = form
         # split slots: batches smaller than this run the FP64 path (the split
         # form pays from ~17 maps of one configuration at B=1024, N=4)
@@ -204,19 +208,23 @@ class Server:
         victim.close()
         return True
 
-    def _acquire(self, key, now):
-        for s in self.slots[key]:
+    def _acquire(self, key, now, form=None):
+        """A free slot of `key` in `form` (the server's form by default),
+        created within the HBM budget if needed; None if there is none."""
+        form = form or ("split" if self.form == "split" else "fp64")
+        mine = [s for s in self.slots[key] if (s.split == (form == "split"))]
+        for s in mine:
             if not s.busy:
                 return s
-        if len(self.slots[key]) >= self.slots_per_config:
+        if len(mine) >= self.slots_per_config:
             return None
         B, N, alpha, J = key
         # size estimate of a new slot; evict idle slots of other configs if needed
-        est = Slot.estimate_bytes(B, N, alpha, J, self.form, self.max_batch, self.batch_bytes)
+        est = Slot.estimate_bytes(B, N, alpha, J, form, self.max_batch, self.batch_bytes)
         while self.used + est > self.budget:
             if not self._evict_one(key):
                 return None
-        s = Slot(key, self.config_tables(B, N, alpha, J), self.device, self.form, self.max_batch, self.batch_bytes,
+        s = Slot(key, self.config_tables(B, N, alpha, J), self.device, form, self.max_batch, self.batch_bytes,
                  priority=size_priority(B) if self.priorities else None, split_min_batch=self.split_min_batch)
         self.slots[key].append(s)
         self.used += s.bytes
@@ -250,7 +258,12 @@ class Server:
                     still.append(r)
                     continue
                 key = (r.B, r.N, r.alpha, r.J)
-                s = self._acquire(key, now)
+                form = None
+                if self.form == "auto":
+                    # a split slot only for a batch the split form serves faster
+                    same = 1 + sum(1 for r2 in waiting if r2.kind == r.kind and (r2.B, r2.N, r2.alpha, r2.J) == key)
+                    form = "split" if same >= self.split_min_batch else "fp64"
+                s = self._acquire(key, now, form)
                 if s is None:
                     still.append(r)
                     continue

@@ -16,6 +16,7 @@ class _StubSlot:
                  split_min_batch=1):
         self.key = key
         self.priority = priority
+        self.split = form == "split"
         self.bytes = _StubSlot.estimate_bytes(*key, form, max_batch, batch_bytes)
         self.busy = False
         self.last_used = 0.0
@@ -87,3 +88,17 @@ def test_size_priority_orders_small_transforms_first(monkeypatch):
     s2 = serving.Server(hbm_budget_bytes=1 << 20)
     monkeypatch.setattr(s2, "config_tables", lambda *k: None)
     assert s2._acquire((64, 2, 2.0, 6), 0.0).priority is None
+
+
+def test_auto_form_picks_split_slots_only_for_large_batches(monkeypatch):
+    """form="auto": a split slot when at least split_min_batch requests of one
+    configuration and kind wait, an FP64 slot otherwise."""
+    monkeypatch.setattr(serving, "Slot", _StubSlot)
+    s = serving.Server(hbm_budget_bytes=1 << 20, form="auto", split_min_batch=3)
+    monkeypatch.setattr(s, "config_tables", lambda *k: None)
+    key = (64, 2, 2.0, 6)
+    a = s._acquire(key, 0.0, "fp64")
+    b = s._acquire(key, 0.0, "split")
+    assert not a.split and b.split and a is not b
+    b.busy = True
+    assert s._acquire(key, 0.0, "split") is not b  # a second split slot (slots_per_config=2)
