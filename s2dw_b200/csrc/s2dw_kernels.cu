@@ -1467,6 +1467,170 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 
 }
 
 // ===========================================================================
+// Prime-factor alpha stages at bl = 2048: n = 2bl-1 = 4095 = 5 * 7 * 9 * 13
+//
+// For the smooth odd length of the full-band scales at B = 2048 the alpha
+// transforms (the c2r of s2dw_core_mod.f90:746-768 and the r2c of :1104-1130,
+// two real rows packed into one complex transform as in the Bluestein
+// engines) run as a Good-Thomas prime-factor DFT: the 4095 values of a row go
+// into shared memory in the 4-D layout L = d1 + 5 d2 + 35 d3 + 315 d4 with
+// input digits d_i = (n u_i) mod R_i, u_i = (4095/R_i)^-1 mod R_i = 4, 2, 2, 9;
+// plain DFTs of length R_i = 5, 7, 9, 13 run along each dimension in place (no
+// twiddles between them); output k sits at digits k mod R_i.  Each small DFT
+// uses the symmetric pairs x_k +- x_{R-k}: (R-1)^2 real-by-complex products
+// instead of R^2.  About 40 FP64 operations per point against ~240 for the
+// 8192-point Bluestein convolution of the general engine.
+// ===========================================================================
+constexpr int PFA_N = 4095, PFA_THREADS = 256;
+
+// cos(2 pi j / R) and sin(2 pi j / R), j < R (local constant tables: with j
+// known after unrolling they fold into immediates)
+template <int R>
+__device__ __forceinline__ void pfa_cs(int j, double &c, double &s);
+template <>
+__device__ __forceinline__ void pfa_cs<5>(int j, double &c, double &s)
+{
+    constexpr double C[5] = {1.0, 0.309016994374947424102, -0.809016994374947424102, -0.809016994374947424102, 0.309016994374947424102};
+    constexpr double S[5] = {0.0, 0.951056516295153572116, 0.587785252292473129169, -0.587785252292473129169, -0.951056516295153572116};
+    c = C[j];
+    s = S[j];
+}
+template <>
+__device__ __forceinline__ void pfa_cs<7>(int j, double &c, double &s)
+{
+    constexpr double C[7] = {1.0, 0.623489801858733530525, -0.222520933956314404289, -0.900968867902419126236, -0.900968867902419126236, -0.222520933956314404289, 0.623489801858733530525};
+    constexpr double S[7] = {0.0, 0.781831482468029808708, 0.974927912181823607018, 0.433883739117558120476, -0.433883739117558120476, -0.974927912181823607018, -0.781831482468029808708};
+    c = C[j];
+    s = S[j];
+}
+template <>
+__device__ __forceinline__ void pfa_cs<9>(int j, double &c, double &s)
+{
+    constexpr double C[9] = {1.0, 0.766044443118978035202, 0.173648177666930348852, -0.5, -0.939692620785908384054, -0.939692620785908384054, -0.5, 0.173648177666930348852, 0.766044443118978035202};
+    constexpr double S[9] = {0.0, 0.642787609686539326323, 0.984807753012208059367, 0.866025403784438646764, 0.342020143325668733044, -0.342020143325668733044, -0.866025403784438646764, -0.984807753012208059367, -0.642787609686539326323};
+    c = C[j];
+    s = S[j];
+}
+template <>
+__device__ __forceinline__ void pfa_cs<13>(int j, double &c, double &s)
+{
+    constexpr double C[13] = {1.0, 0.885456025653209895900, 0.568064746731155802512, 0.120536680255323053349, -0.354604887042535625970, -0.748510748171101098635, -0.970941817426052027157, -0.970941817426052027157, -0.748510748171101098635, -0.354604887042535625970, 0.120536680255323053349, 0.568064746731155802512, 0.885456025653209895900};
+    constexpr double S[13] = {0.0, 0.464723172043768545656, 0.822983865893656394580, 0.992708874098053992801, 0.935016242685414823440, 0.663122658240795202377, 0.239315664287557767149, -0.239315664287557767149, -0.663122658240795202377, -0.935016242685414823440, -0.992708874098053992801, -0.822983865893656394580, -0.464723172043768545656};
+    c = C[j];
+    s = S[j];
+}
+
+// In-place DFT of length R (odd) with exp(SIGN 2 pi i k m / R):
+// y_m = x_0 + sum_k (x_k + x_{R-k}) cos + SIGN i sum_k (x_k - x_{R-k}) sin.
+template <int R, int SIGN>
+__device__ __forceinline__ void pfa_dft(double2 (&x)[R])
+{
+    constexpr int H = (R - 1) / 2;
+    double2 ap[H], am[H];
+    double2 y0 = x[0];
+#pragma unroll
+    for (int k = 1; k <= H; k++) {
+        ap[k - 1] = cadd(x[k], x[R - k]);
+        am[k - 1] = csub(x[k], x[R - k]);
+        y0 = cadd(y0, ap[k - 1]);
+    }
+    const double2 x0 = x[0];
+    x[0] = y0;
+#pragma unroll
+    for (int m = 1; m <= H; m++) {
+        double2 P = x0, Q = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int k = 1; k <= H; k++) {
+            double c, sn;
+            pfa_cs<R>((k * m) % R, c, sn);
+            P.x = fma(ap[k - 1].x, c, P.x);
+            P.y = fma(ap[k - 1].y, c, P.y);
+            Q.x = fma(am[k - 1].x, sn, Q.x);
+            Q.y = fma(am[k - 1].y, sn, Q.y);
+        }
+        // SIGN i Q
+        const double2 iq = SIGN > 0 ? make_double2(-Q.y, Q.x) : make_double2(Q.y, -Q.x);
+        x[m] = cadd(P, iq);
+        x[R - m] = csub(P, iq);
+    }
+}
+
+// DFTs of length R along the dimension of stride S of the 4-D layout.
+template <int R, int S, int SIGN>
+__device__ __forceinline__ void pfa_stage(double2 *sm, int t)
+{
+    for (int d = t; d < PFA_N / R; d += PFA_THREADS) {
+        const int base = (d % S) + (d / S) * (S * R);
+        double2 x[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) x[r] = sm[base + r * S];
+        pfa_dft<R, SIGN>(x);
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[base + r * S] = x[r];
+    }
+}
+
+__device__ __forceinline__ int pfa_in_pos(int n)
+{
+    return (n * 4) % 5 + 5 * ((n * 2) % 7) + 35 * ((n * 2) % 9) + 315 * ((n * 9) % 13);
+}
+__device__ __forceinline__ int pfa_out_pos(int k) { return k % 5 + 5 * (k % 7) + 35 * (k % 9) + 315 * (k % 13); }
+
+// One CTA per (g, b pair): the two real rows of the pair, as fft_large_kernel.
+template <int MODE>
+__global__ void __launch_bounds__(PFA_THREADS, 3) pfa_alpha_kernel(CztArgs a)
+{
+    static_assert(MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA, "alpha stages only");
+    constexpr int SIGN = MODE == CZT_ANA_ALPHA ? +1 : -1;
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = PFA_N;  // n = 2 bl - 1
+    const int g = blockIdx.y, rr = blockIdx.x;
+    for (int m = t; m < n; m += PFA_THREADS) {
+        double2 z;
+        if (MODE == CZT_ANA_ALPHA) {  // Hermitian completion in m, as fft_large_kernel
+            const bool lo = m < bl;
+            const double2 *p = a.in_c + ((size_t)g * bl + (lo ? m : n - m)) * (2 * bl) + 2 * rr;
+            double2 x1, x2;
+            ld_pair(p, x1, x2);
+            if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
+            if (m == 0) { x1.y = 0.0; x2.y = 0.0; }
+            z = make_double2(x1.x - x2.y, x1.y + x2.x);
+        } else {  // z = w(:, b1) + i w(:, b2)
+            const double *p = a.in_r + (size_t)m + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            z = make_double2(p[0], p[n]);
+        }
+        smem[pfa_in_pos(m)] = z;
+    }
+    __syncthreads();
+    pfa_stage<5, 1, SIGN>(smem, t);
+    __syncthreads();
+    pfa_stage<7, 5, SIGN>(smem, t);
+    __syncthreads();
+    pfa_stage<9, 35, SIGN>(smem, t);
+    __syncthreads();
+    pfa_stage<13, 315, SIGN>(smem, t);
+    __syncthreads();
+    if (MODE == CZT_ANA_ALPHA) {
+        for (int k = t; k < n; k += PFA_THREADS) {
+            const double2 y = smem[pfa_out_pos(k)];
+            double *p = a.out_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            p[0] = y.x;
+            p[n] = y.y;
+        }
+    } else {  // even / odd split of the two real rows' spectra, m < bl
+        const double hh = 0.5 * a.scale;
+        for (int m = t; m < bl; m += PFA_THREADS) {
+            const double2 Z = smem[pfa_out_pos(m)];
+            const double2 Zc = cconj(smem[pfa_out_pos(m == 0 ? 0 : n - m)]);
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+}
+
+// ===========================================================================
 // Small kernels
 // ===========================================================================
 __global__ void zero_kernel(double *p, long long n)
@@ -1756,6 +1920,27 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
     return set_error(S2DWC_ERROR_ARG_INVALID, "unknown transform mode %d", a.mode);
 }
 
+template <int MODE>
+static int launch_pfa(const CztArgs &a, cudaStream_t s)
+{
+    const size_t smem = sizeof(double2) * PFA_N;
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(pfa_alpha_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        attr[dev] = true;
+    }
+    const dim3 grid(a.bl, a.rows / a.bl);  // (b pair, g)
+    pfa_alpha_kernel<MODE><<<grid, PFA_THREADS, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048
+void set_pfa(bool on) { g_pfa = on; }
+
 static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
 static bool g_large_2048 = true;  // M = 2048 transforms on the one-row-per-CTA engines
 static bool g_alpha_prefetch = true;  // contiguous-input stages: persistent kernel with prefetched input
@@ -1794,6 +1979,10 @@ void set_alpha_prefetch(bool on) { g_alpha_prefetch = on; }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
+    if (g_pfa && a.bl == 2048 && 2 * a.bl - 1 == PFA_N && a.rows % a.bl == 0) {
+        if (a.mode == CZT_ANA_ALPHA) return launch_pfa<CZT_ANA_ALPHA>(a, s);
+        if (a.mode == CZT_SYN_ALPHA) return launch_pfa<CZT_SYN_ALPHA>(a, s);
+    }
     const int M = a.czt.M;
     if (M < 16 || M > 8192 || (M & (M - 1)))
         return set_error(S2DWC_ERROR_SIZE_INVALID, "transform size %d unsupported", M);

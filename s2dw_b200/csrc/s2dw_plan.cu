@@ -1213,6 +1213,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     {
         const char *l2 = getenv("S2DW_LARGE_2048");
         set_large_2048(l2 ? atoi(l2) != 0 : true);
+        const char *pf = getenv("S2DW_PFA");
+        set_pfa(pf ? atoi(pf) != 0 : true);
     }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");

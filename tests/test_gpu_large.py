@@ -128,3 +128,43 @@ def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
     np.testing.assert_array_equal(out["1"][0], out["0"][0])
     np.testing.assert_array_equal(out["1"][1], out["0"][1])
     assert np.abs(out["1"][1].T - flm).max() <= 1e-10
+
+
+@pytest.mark.gpu
+def test_prime_factor_alpha_matches_bluestein(monkeypatch):
+    """At bl = 2048 the alpha stages run as a prime-factor DFT of
+    4095 = 5*7*9*13 (S2DW_PFA=1, the default) instead of an 8192-point
+    Bluestein convolution (S2DW_PFA=0): both are the same transform, so the
+    coefficients of every scale and the synthesised flm agree to rounding
+    (1e-13 relative)."""
+    import torch
+
+    from s2dw_b200.device import Plan
+
+    B, N, alpha = 2048, 2, 2.0
+    t = transform_setup(B, N, alpha)
+    flm = gaussian_flm(B, seed=5, power=1.2)
+    d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
+    out = {}
+    for pf in ("1", "0"):
+        monkeypatch.setenv("S2DW_PFA", pf)
+        p = Plan(B, N, alpha, t["J"])
+        p.set_tables(t["K_gamma"], t["Phi2"], t["Slm"], t["bl_scoeff"])
+        w = torch.empty(p.wav_size, dtype=torch.float64, device="cuda")
+        sc = torch.empty(max(1, t["bl_scoeff"] ** 2), dtype=torch.complex128, device="cuda")
+        f = torch.empty_like(d_flm)
+        p.analysis(d_flm, w, sc)
+        p.synthesis(w, sc, f)
+        torch.cuda.synchronize()
+        out[pf] = (w.cpu().numpy(), f.cpu().numpy(), p.wav_offsets)
+        p.close()
+    monkeypatch.setenv("S2DW_PFA", "1")
+    Plan(16, 2, 2.0, core.s2dw_core_comp_Jmax(16, 2.0)).close()  # restore the default for later tests
+    offs = out["1"][2]
+    for j in range(t["J"] + 1):
+        a, b = out["1"][0][offs[j]:offs[j + 1]], out["0"][0][offs[j]:offs[j + 1]]
+        if np.abs(b).max() > 0:
+            assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max(), j
+    fa, fb = out["1"][1], out["0"][1]
+    assert np.abs(fa - fb).max() <= 1e-13 * np.abs(fb).max()
+    assert np.abs(fa.T - flm).max() <= 1e-10 * np.abs(flm).max()
