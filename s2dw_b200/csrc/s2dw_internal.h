@@ -222,7 +222,11 @@ int launch_mwalk(const MwalkArgs &a, cudaStream_t s);
 int launch_czt(const CztArgs &a, cudaStream_t s);
 void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread, 0 = general engine only
 void set_large_2048(bool on);  // M = 2048 transforms on the one-row-per-CTA engines (default on)
-void set_pfa(bool on);  // prime-factor alpha stages at bl = 2048 (default on)
+void set_pfa(bool on);  // prime-factor alpha stages at bl = 2048 and 1024 (default on)
+void set_pfa2047_threads(int n);  // threads per CTA of the length-2047 kernel (128 or 256)
+// Builds, once per device, the constant table of the length-2047 alpha stages
+// (the current device; synchronises).  Plan creation calls it, never a capture.
+int pfa_prepare();
 void set_alpha_prefetch(bool on);  // synthesis alpha / analysis beta stages: persistent kernel with prefetched input (default on)
 void set_walk_variants(int lwalk, int mwalk);  // tile shape / occupancy variants of the contraction kernels
 int launch_zero(double *p, long long n, cudaStream_t s);

@@ -1630,6 +1630,228 @@ __global__ void __launch_bounds__(PFA_THREADS, 3) pfa_alpha_kernel(CztArgs a)
     }
 }
 
+template <>
+__device__ __forceinline__ void pfa_cs<11>(int j, double &c, double &s)
+{
+    constexpr double C[11] = {
+        1.00000000000000000000, 0.841253532831181168862, 0.415415013001886425529, -0.142314838273285140444,
+        -0.654860733945285064057, -0.959492973614497389890, -0.959492973614497389890, -0.654860733945285064057,
+        -0.142314838273285140444, 0.415415013001886425529, 0.841253532831181168862};
+    constexpr double S[11] = {
+        0.0, 0.540640817455597582108, 0.909631995354518371412, 0.989821441880932732376, 0.755749574354258283774,
+        0.281732556841429697711, -0.281732556841429697711, -0.755749574354258283774, -0.989821441880932732376,
+        -0.909631995354518371412, -0.540640817455597582108};
+    c = C[j];
+    s = S[j];
+}
+template <>
+__device__ __forceinline__ void pfa_cs<23>(int j, double &c, double &s)
+{
+    constexpr double C[23] = {
+        1.00000000000000000000, 0.962917287347799295015, 0.854419404546488552548, 0.682553143218654082875,
+        0.460065037731152126042, 0.203456013052633789878, -0.0682424133646709759212, -0.334879612170986151958,
+        -0.576680322114867141251, -0.775711290704419807041, -0.917211301505453017844, -0.990685946036330752342,
+        -0.990685946036330752342, -0.917211301505453017844, -0.775711290704419807041, -0.576680322114867141251,
+        -0.334879612170986151958, -0.0682424133646709759212, 0.203456013052633789878, 0.460065037731152126042,
+        0.682553143218654082875, 0.854419404546488552548, 0.962917287347799295015};
+    constexpr double S[23] = {
+        0.0, 0.269796771157024271245, 0.519583950035433578133, 0.730835964278124101651, 0.887885218402375234984,
+        0.979084087682322875633, 0.997668769190539198454, 0.942260922118820495618, 0.816969893010442016973,
+        0.631087944326052789367, 0.398401089846241457998, 0.136166649096246590761, -0.136166649096246590761,
+        -0.398401089846241457998, -0.631087944326052789367, -0.816969893010442016973, -0.942260922118820495618,
+        -0.997668769190539198454, -0.979084087682322875633, -0.887885218402375234984, -0.730835964278124101651,
+        -0.519583950035433578133, -0.269796771157024271245};
+    c = C[j];
+    s = S[j];
+}
+
+// In-place-input DFT of length R (odd), outputs written to out[base + m S]:
+// the symmetric pairs overwrite x (x_k <- x_k + x_{R-k}, x_{R-k} <- x_k - x_{R-k}),
+// which keeps the registers of a long DFT (R = 23) to about R complex values.
+template <int R, int SIGN>
+__device__ __forceinline__ void pfa_dft_out(double2 (&x)[R], double2 *out, int base, int S)
+{
+    constexpr int H = (R - 1) / 2;
+    const double2 x0 = x[0];
+    double2 y0 = x0;
+#pragma unroll
+    for (int k = 1; k <= H; k++) {
+        const double2 p = cadd(x[k], x[R - k]), q = csub(x[k], x[R - k]);
+        x[k] = p;
+        x[R - k] = q;
+        y0 = cadd(y0, p);
+    }
+    out[base] = y0;
+#pragma unroll
+    for (int m = 1; m <= H; m++) {
+        double2 P = x0, Q = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int k = 1; k <= H; k++) {
+            double c, sn;
+            pfa_cs<R>((k * m) % R, c, sn);
+            P.x = fma(x[k].x, c, P.x);
+            P.y = fma(x[k].y, c, P.y);
+            Q.x = fma(x[R - k].x, sn, Q.x);
+            Q.y = fma(x[R - k].y, sn, Q.y);
+        }
+        const double2 iq = SIGN > 0 ? make_double2(-Q.y, Q.x) : make_double2(Q.y, -Q.x);
+        out[base + m * S] = cadd(P, iq);
+        out[base + (R - m) * S] = csub(P, iq);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Prime-factor alpha stages at bl = 1024: n = 2047 = 23 * 89
+//
+// Good-Thomas over 23 x 89 as above (layout L = d1 + 23 d2, input digits
+// (n 15) mod 23 and (n 31) mod 89, output digits k mod 23, k mod 89).  The
+// length-89 DFTs run by Rader's algorithm: with the primitive root g = 3,
+// y_{g^r} = x_0 + sum_q x_{g^-q} w_{r-q}, w_j = exp(SIGN 2 pi i g^j / 89), a cyclic
+// convolution of length 88 done as a forward DFT of 88 = 8 x 11 (Good-Thomas
+// again: radix-8 in registers, then length 11), a product with the DFT of w
+// (g_rader_w, built once per device by rader_init_kernel), and the inverse
+// DFT; y_0 = x_0 + the convolution input's sum.  About 60 FP64 operations per
+// point against ~240 for the 4096-point Bluestein convolution.
+// ---------------------------------------------------------------------------
+constexpr int PFB_N = 2047;
+constexpr int PFB_P = 25;              // pitch of d2 in the shared row
+constexpr int PFB_XS = PFB_P * 89;     // shared row size
+constexpr int PFB_SP = 98;             // pitch of a Rader column (positions i + 9 j, i < 8, j < 11)
+
+// per position L = i + 8 j of the 88-layout (input digits (q 3) mod 8,
+// (q 7) mod 11): the length-89 index g^-q whose value goes there, and g^q,
+// where the convolution's output at L goes
+__constant__ int c_rader_src[88] = {
+    1, 77, 55, 52, 88, 12, 34, 37, 32, 61, 69, 62, 57, 28, 20, 27, 45, 83, 72, 26, 44, 6, 17, 63, 16, 75, 79, 31,
+    73, 14, 10, 58, 67, 86, 36, 13, 22, 3, 53, 76, 8, 82, 84, 60, 81, 7, 5, 29, 78, 43, 18, 51, 11, 46, 71, 38, 4,
+    41, 42, 30, 85, 48, 47, 59, 39, 66, 9, 70, 50, 23, 80, 19, 2, 65, 21, 15, 87, 24, 68, 74, 64, 33, 49, 35, 25,
+    56, 40, 54};
+__constant__ int c_rader_dst[88] = {
+    1, 37, 34, 12, 88, 52, 55, 77, 64, 54, 40, 56, 25, 35, 49, 33, 2, 74, 68, 24, 87, 15, 21, 65, 39, 19, 80, 23,
+    50, 70, 9, 66, 4, 59, 47, 48, 85, 30, 42, 41, 78, 38, 71, 46, 11, 51, 18, 43, 8, 29, 5, 7, 81, 60, 84, 82, 67,
+    76, 53, 3, 22, 13, 36, 86, 16, 58, 10, 14, 73, 31, 79, 75, 45, 63, 17, 6, 44, 26, 72, 83, 32, 27, 20, 28, 57,
+    62, 69, 61};
+// [0]: SIGN -1, [1]: SIGN +1; entry L_out(k) = k mod 8 + 8 (k mod 11) holds
+// (1/88) sum_j w_j exp(-2 pi i j k / 88)
+__device__ double2 g_rader_w[2][88];
+
+__global__ void rader_init_kernel()
+{
+    const int sgn = blockIdx.x ? 1 : -1, k = threadIdx.x;
+    if (k >= 88) return;
+    double re = 0.0, im = 0.0;
+    int gj = 1;  // 3^j mod 89
+    for (int j = 0; j < 88; j++) {
+        double s1, c1, s2, c2;
+        sincospi(2.0 * sgn * gj / 89.0, &s1, &c1);
+        sincospi(-2.0 * ((j * k) % 88) / 88.0, &s2, &c2);
+        re += c1 * c2 - s1 * s2;
+        im += c1 * s2 + s1 * c2;
+        gj = (gj * 3) % 89;
+    }
+    g_rader_w[blockIdx.x][k % 8 + 8 * (k % 11)] = make_double2(re / 88.0, im / 88.0);
+}
+
+template <int MODE, int NT>
+__global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(CztArgs a)
+{
+    static_assert(MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA, "alpha stages only");
+    constexpr int SIGN = MODE == CZT_ANA_ALPHA ? +1 : -1;
+    extern __shared__ double2 smem[];
+    // the row in layout d1 + 25 d2 (pitch 25: conflict-free shared-memory
+    // access for the length-23 DFTs, two-way for the output gather); the 23
+    // Rader convolutions in layout i + 9 j (pitch 98 per column)
+    double2 *X = smem;
+    double2 *Sc = smem + PFB_XS;
+    double2 *X0 = Sc + 23 * PFB_SP;
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = PFB_N;  // n = 2 bl - 1
+    const int g = blockIdx.y, rr = blockIdx.x;
+    for (int m = t; m < n; m += NT) {
+        double2 z;
+        if (MODE == CZT_ANA_ALPHA) {
+            const bool lo = m < bl;
+            const double2 *p = a.in_c + ((size_t)g * bl + (lo ? m : n - m)) * (2 * bl) + 2 * rr;
+            double2 x1, x2;
+            ld_pair(p, x1, x2);
+            if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
+            if (m == 0) { x1.y = 0.0; x2.y = 0.0; }
+            z = make_double2(x1.x - x2.y, x1.y + x2.x);
+        } else {
+            const double *p = a.in_r + (size_t)m + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            z = make_double2(p[0], p[n]);
+        }
+        X[(m * 15) % 23 + PFB_P * ((m * 31) % 89)] = z;
+    }
+    __syncthreads();
+    // length-23 DFTs along d1
+    for (int d2 = t; d2 < 89; d2 += NT) {
+        double2 x[23];
+#pragma unroll
+        for (int r = 0; r < 23; r++) x[r] = X[PFB_P * d2 + r];
+        pfa_dft_out<23, SIGN>(x, X, PFB_P * d2, 1);
+    }
+    __syncthreads();
+    // length-89 DFTs along d2 (column c1) by Rader: forward length-8 DFTs of
+    // the permuted inputs
+    for (int u = t; u < 23 * 11; u += NT) {
+        const int c1 = u / 11, j = u % 11;
+        double2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = X[c1 + PFB_P * c_rader_src[i + 8 * j]];
+        Dft<8, -1>::run(v);
+#pragma unroll
+        for (int i = 0; i < 8; i++) Sc[c1 * PFB_SP + i + 9 * j] = v[i];
+        if (j == 0) X0[c1] = X[c1];
+    }
+    __syncthreads();
+    // forward length-11 DFTs, product with the DFT of w, inverse length-11
+    for (int u = t; u < 23 * 8; u += NT) {
+        const int c1 = u / 8, i = u % 8;
+        double2 v[11];
+#pragma unroll
+        for (int jj = 0; jj < 11; jj++) v[jj] = Sc[c1 * PFB_SP + i + 9 * jj];
+        pfa_dft<11, -1>(v);
+        if (i == 0) X[c1] = cadd(X0[c1], v[0]);  // y_0 = x_0 + sum of the other inputs
+#pragma unroll
+        for (int kk = 0; kk < 11; kk++) v[kk] = cmul(v[kk], g_rader_w[SIGN > 0 ? 1 : 0][i + 8 * kk]);
+        pfa_dft<11, +1>(v);
+#pragma unroll
+        for (int jj = 0; jj < 11; jj++) Sc[c1 * PFB_SP + i + 9 * jj] = v[jj];
+    }
+    __syncthreads();
+    // inverse length-8 DFTs; y_{g^q} = x_0 + convolution
+    for (int u = t; u < 23 * 11; u += NT) {
+        const int c1 = u / 11, j = u % 11;
+        double2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = Sc[c1 * PFB_SP + i + 9 * j];
+        Dft<8, +1>::run(v);
+        const double2 x0 = X0[c1];
+#pragma unroll
+        for (int i = 0; i < 8; i++) X[c1 + PFB_P * c_rader_dst[i + 8 * j]] = cadd(x0, v[i]);
+    }
+    __syncthreads();
+    if (MODE == CZT_ANA_ALPHA) {
+        for (int k = t; k < n; k += NT) {
+            const double2 y = X[k % 23 + PFB_P * (k % 89)];
+            double *p = a.out_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            p[0] = y.x;
+            p[n] = y.y;
+        }
+    } else {
+        const double hh = 0.5 * a.scale;
+        for (int m = t; m < bl; m += NT) {
+            const int mc = m == 0 ? 0 : n - m;
+            const double2 Z = X[m % 23 + PFB_P * (m % 89)];
+            const double2 Zc = cconj(X[mc % 23 + PFB_P * (mc % 89)]);
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+}
+
 // ===========================================================================
 // Small kernels
 // ===========================================================================
@@ -1938,8 +2160,43 @@ static int launch_pfa(const CztArgs &a, cudaStream_t s)
     return S2DWC_OK;
 }
 
-static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048
+template <int MODE, int NT>
+static int launch_pfa2047(const CztArgs &a, cudaStream_t s)
+{
+    const size_t smem = sizeof(double2) * (PFB_XS + 23 * PFB_SP + 23);
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(pfa2047_alpha_kernel<MODE, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        attr[dev] = true;
+    }
+    const dim3 grid(a.bl, a.rows / a.bl);  // (b pair, g)
+    pfa2047_alpha_kernel<MODE, NT><<<grid, NT, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+static bool g_rader_ready[64] = {false};
+
+int pfa_prepare()
+{
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(S2DWC_ERROR_ARG_INVALID, "device index %d", dev);
+    if (g_rader_ready[dev]) return S2DWC_OK;
+    rader_init_kernel<<<2, 96>>>();
+    S2DW_CUDA_TRY(cudaGetLastError());
+    S2DW_CUDA_TRY(cudaStreamSynchronize(0));
+    g_rader_ready[dev] = true;
+    return S2DWC_OK;
+}
+
+static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048 and 1024
+static int g_pfa2047_threads = 128;
 void set_pfa(bool on) { g_pfa = on; }
+void set_pfa2047_threads(int n) { g_pfa2047_threads = n == 256 ? 256 : 128; }
 
 static int g_fft_values = 8;  // values per thread of the general FFT engine (8 or 16)
 static bool g_large_2048 = true;  // M = 2048 transforms on the one-row-per-CTA engines
@@ -1982,6 +2239,19 @@ int launch_czt(const CztArgs &a, cudaStream_t s)
     if (g_pfa && a.bl == 2048 && 2 * a.bl - 1 == PFA_N && a.rows % a.bl == 0) {
         if (a.mode == CZT_ANA_ALPHA) return launch_pfa<CZT_ANA_ALPHA>(a, s);
         if (a.mode == CZT_SYN_ALPHA) return launch_pfa<CZT_SYN_ALPHA>(a, s);
+    }
+    if (g_pfa && a.bl == 1024 && 2 * a.bl - 1 == PFB_N && a.rows % a.bl == 0) {
+        int dev = 0;
+        S2DW_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64 || !g_rader_ready[dev])
+            return set_error(S2DWC_ERROR_NOT_INIT, "the length-2047 alpha tables are not built on device %d", dev);
+        if (g_pfa2047_threads == 128) {
+            if (a.mode == CZT_ANA_ALPHA) return launch_pfa2047<CZT_ANA_ALPHA, 128>(a, s);
+            if (a.mode == CZT_SYN_ALPHA) return launch_pfa2047<CZT_SYN_ALPHA, 128>(a, s);
+        } else {
+            if (a.mode == CZT_ANA_ALPHA) return launch_pfa2047<CZT_ANA_ALPHA, 256>(a, s);
+            if (a.mode == CZT_SYN_ALPHA) return launch_pfa2047<CZT_SYN_ALPHA, 256>(a, s);
+        }
     }
     const int M = a.czt.M;
     if (M < 16 || M > 8192 || (M & (M - 1)))

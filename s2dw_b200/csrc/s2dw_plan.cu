@@ -400,6 +400,7 @@ int plan_build(s2dwc_plan *p)
         p->mw_ntiles.push_back(p->bl[j] - p->blo[j] - 1 > 0 ? (int)tl.size() : 0);
     }
     if (p->dry) return S2DWC_OK;
+    if (std::find(p->bl.begin(), p->bl.end(), 1024) != p->bl.end() && (st = pfa_prepare())) return st;
     p->streams.resize(J + 1);
     p->ev_join.resize(J + 1);
     for (int j = 0; j <= J; j++) {
@@ -1215,6 +1216,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         set_large_2048(l2 ? atoi(l2) != 0 : true);
         const char *pf = getenv("S2DW_PFA");
         set_pfa(pf ? atoi(pf) != 0 : true);
+        const char *pt = getenv("S2DW_PFA2047_THREADS");
+        set_pfa2047_threads(pt ? atoi(pt) : 128);
     }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");
