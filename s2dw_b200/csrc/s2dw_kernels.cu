@@ -144,12 +144,12 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
         }
     }
 
-    double e[S], ep[S];
+    double x[2][S];
     double2 acc[2][S][NP];
 #pragma unroll
     for (int s = 0; s < S; s++) {
-        e[s] = 0.0;
-        ep[s] = 0.0;
+        x[0][s] = 0.0;
+        x[1][s] = 0.0;
 #pragma unroll
         for (int q = 0; q < NP; q++) acc[0][s][q] = acc[1][s][q] = make_double2(0.0, 0.0);
     }
@@ -158,28 +158,44 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
     const int rampEnd = min(max(p0 + 31, m0 + WS - 1), bl - 1);
     const int nchunks = (bl - lstart + LW_CH - 1) / LW_CH;
 
+    // Staging: the 16-byte pieces of a chunk's rows go to the threads in a
+    // fixed pattern (piece column from the thread index, rows in passes), so
+    // that a copy costs a row bound check and one address computation.
+    static_assert(LW_W * 32 == 128 && LW_CH % 8 == 0, "staging pattern assumes 128 threads");
     auto stage = [&](int c, int buf) {
         const int lc = lstart + c * LW_CH;
         double *b = lsm + buf * L::BUF;
-        // a(l, m') and a(l, m): 32 and WS doubles per row
-        for (int i = tid; i < LW_CH * (16 + WS / 2); i += blockDim.x) {
-            const int li = i / (16 + WS / 2), r = i % (16 + WS / 2), l = lc + li;
-            if (l >= bl) continue;
-            if (r < 16) cp16(b + L::AP_OFF + li * 32 + 2 * r, a.Acoef + (size_t)l * Bp + p0 + 2 * r);
-            else cp16(b + L::AM_OFF + li * WS + 2 * (r - 16), a.Acoef + (size_t)l * Bp + m0 + 2 * (r - 16));
+        const int pc = tid & 15;  // piece of a 32-double row
+        // a(l, m'): 16 pieces per row, 8 rows per pass
+#pragma unroll
+        for (int i = 0; i < LW_CH / 8; i++) {
+            const int li = (tid >> 4) + 8 * i, l = lc + li;
+            if (l < bl) cp16(b + L::AP_OFF + li * 32 + 2 * pc, a.Acoef + (size_t)l * Bp + p0 + 2 * pc);
+        }
+        // a(l, m): WS/2 pieces per row
+        constexpr int AMP = WS / 2, AMR = 128 / AMP;
+#pragma unroll
+        for (int i = 0; i < (LW_CH + AMR - 1) / AMR; i++) {
+            const int li = tid / AMP + AMR * i, l = lc + li;
+            if (li < LW_CH && l < bl)
+                cp16(b + L::AM_OFF + li * WS + 2 * (tid % AMP), a.Acoef + (size_t)l * Bp + m0 + 2 * (tid % AMP));
         }
         if (lc + LW_CH - 1 > blo) {
-            for (int i = tid; i < LW_CH * (NP * 16 + WS); i += blockDim.x) {
-                const int li = i / (NP * 16 + WS), r = i % (NP * 16 + WS), l = lc + li;
-                if (l >= bl || l <= blo) continue;
-                if (r < NP * 16) {
-                    const int q = r >> 4, c2 = r & 15;
-                    cp16(b + L::G_OFF + (li * NP + q) * 32 + 2 * c2,
-                         a.G + ((size_t)(l - blo - 1) * NP + q) * Gs + p0 + 2 * c2);
-                } else {
-                    const int c1 = r - NP * 16;
-                    cp16(b + L::F_OFF + 2 * (li * WS + c1), a.F + (size_t)l * Bp + m0 + c1);
-                }
+            // G(l, m', q): rows r = li NP + q of 16 pieces, 8 rows per pass
+#pragma unroll
+            for (int i = 0; i < LW_CH * NP / 8; i++) {
+                const int r = (tid >> 4) + 8 * i, l = lc + r / NP;
+                if (l > blo && l < bl)
+                    cp16(b + L::G_OFF + r * 32 + 2 * pc,
+                         a.G + ((long long)(lc - blo - 1) * NP + r) * Gs + p0 + 2 * pc);
+            }
+            // F(l, m): WS pieces (complex values) per row
+            constexpr int FR = 128 / WS;
+#pragma unroll
+            for (int i = 0; i < (LW_CH + FR - 1) / FR; i++) {
+                const int li = tid / WS + FR * i, l = lc + li;
+                if (li < LW_CH && l > blo && l < bl)
+                    cp16(b + L::F_OFF + 2 * (li * WS + tid % WS), a.F + (size_t)l * Bp + m0 + tid % WS);
             }
         }
     };
@@ -197,10 +213,11 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
         const double *Amr = b + L::AM_OFF + li * WS + w * S;
 #pragma unroll
         for (int s = 0; s < S; s++) {
-            if (inj && l == l0[s]) e[s] = st[s];
+            if (inj && l == l0[s]) x[PAR][s] = st[s];
+            const double cur = x[PAR][s];
             if (accum) {
                 const double2 F = Fr[s];
-                const double xr = e[s] * F.x, xi = e[s] * F.y;
+                const double xr = cur * F.x, xi = cur * F.y;
 #pragma unroll
                 for (int q = 0; q < NP; q++) {
                     acc[PAR][s][q].x = fma(xr, g[q], acc[PAR][s][q].x);
@@ -208,9 +225,7 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
                 }
             }
             const double p = Amr[s] * ap;
-            const double en = fma(-p, e[s], -ep[s]);
-            ep[s] = e[s];
-            e[s] = en;
+            x[PAR ^ 1][s] = fma(-p, cur, -x[PAR ^ 1][s]);
         }
     };
     using P0 = std::integral_constant<int, 0>;
@@ -243,15 +258,15 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
         if (Kw > 0) {  // keep scaled values in range (warp-uniform)
             double mx = 0.0;
 #pragma unroll
-            for (int s = 0; s < S; s++) mx = fmax(mx, fmax(fabs(e[s]), fabs(ep[s])));
+            for (int s = 0; s < S; s++) mx = fmax(mx, fmax(fabs(x[0][s]), fabs(x[1][s])));
             mx = warp_max(mx);
             if (mx > ldexp(1.0, S2DW_RENORM_EXP)) {
                 const int R = min(S2DW_RENORM_EXP, Kw);
                 const double f = ldexp(1.0, -R);
 #pragma unroll
                 for (int s = 0; s < S; s++) {
-                    e[s] *= f;
-                    ep[s] *= f;
+                    x[0][s] *= f;
+                    x[1][s] *= f;
 #pragma unroll
                     for (int q = 0; q < NP; q++) {
                         acc[0][s][q] = cscale(acc[0][s][q], f);
@@ -428,31 +443,39 @@ __device__ __forceinline__ void mwalk_body(const MwalkArgs &a)
 
     const int ctop = MH / MW_CH;  // chunks ctop, ctop-1, ..., 0 cover m' = MH .. 0
 
+    // Staging: a fixed pattern of 16-byte pieces per thread (see lwalk).  The
+    // rows of l >= bl and of m >= bl are never copied: they are zeroed once
+    // here, in both buffers, so that the idle lanes and pairs walk zeros.
+    static_assert(MW_W * 32 == 128 && MW_CH == 8, "staging pattern assumes 128 threads, 8 m' per chunk");
+    const int nt = min(32, bl - lbase), nu = min(WQ, bl - mbase);
+    if (nt < 32 || nu < WQ) {
+        for (int i = tid; i < 2 * L::BUF; i += blockDim.x) {
+            const int r = i % L::BUF;
+            bool idle;
+            if (r < L::B_OFF) idle = ((r - L::V_OFF) / (2 * MW_CH)) % WQ >= nu;
+            else if (r < L::G_OFF) idle = (r - L::B_OFF) / MW_RS >= nt;
+            else idle = ((r - L::G_OFF) / MW_RS) % 32 >= nt;
+            if (idle) msm[i] = 0.0;
+        }
+    }
     auto stage = [&](int c, int buf) {
         double *b = msm + buf * L::BUF;
         const int c0 = c * MW_CH;
-        // rows of b(l, m') and G(l, m', q): MW_CH/2 copies per row
-        for (int i = tid; i < (1 + NP) * 32 * (MW_CH / 2); i += blockDim.x) {
-            const int k = i % (MW_CH / 2), row = i / (MW_CH / 2), t = row % 32, q = row / 32;
-            const int ll = lbase + t;
-            double *dst = (q == 0) ? b + L::B_OFF + t * MW_RS + 2 * k
-                                   : b + L::G_OFF + ((q - 1) * 32 + t) * MW_RS + 2 * k;
-            if (ll < bl) {
-                const double *src = (q == 0) ? a.Bcoef + (size_t)ll * Bp + c0 + 2 * k
-                                             : a.G + ((size_t)(ll - blo - 1) * NP + (q - 1)) * Gs + c0 + 2 * k;
-                cp16(dst, src);
-            } else {
-                dst[0] = 0.0;
-                dst[1] = 0.0;
-            }
+        // b(l, m') and G(l, m', q): 4 pieces per row, one row per 4 threads
+        const int t = tid >> 2, k = tid & 3, ll = lbase + t;
+        if (ll < bl) {
+            cp16(b + L::B_OFF + t * MW_RS + 2 * k, a.Bcoef + (size_t)ll * Bp + c0 + 2 * k);
+#pragma unroll
+            for (int q = 0; q < NP; q++)
+                cp16(b + L::G_OFF + (q * 32 + t) * MW_RS + 2 * k,
+                     a.G + ((size_t)(ll - blo - 1) * NP + q) * Gs + c0 + 2 * k);
         }
-        // V2f(m, m', q) for the tile's m: MW_CH complex per (q, m)
-        for (int i = tid; i < NP * WQ * MW_CH; i += blockDim.x) {
-            const int k = i % MW_CH, r = i / MW_CH, u = r % WQ, q = r / WQ;
-            const int m = mbase + u;
-            double *dst = b + L::V_OFF + 2 * ((q * WQ + u) * MW_CH + k);
-            if (m < bl) cp16(dst, a.V2f + ((size_t)q * bl + m) * Vs + c0 + k);
-            else { dst[0] = 0.0; dst[1] = 0.0; }
+        // V2f(m, m', q): MW_CH pieces (complex values) per (q, m) row
+#pragma unroll
+        for (int i = 0; i < NP * WQ * MW_CH / 128; i++) {
+            const int f = tid + 128 * i, kk = f % MW_CH, r = f / MW_CH, u = r % WQ, q = r / WQ;
+            if (mbase + u < bl)
+                cp16(b + L::V_OFF + 2 * (r * MW_CH + kk), a.V2f + ((size_t)q * bl + mbase + u) * Vs + c0 + kk);
         }
     };
 

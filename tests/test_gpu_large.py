@@ -131,17 +131,19 @@ def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
 
 
 @pytest.mark.gpu
-def test_prime_factor_alpha_matches_bluestein(monkeypatch):
-    """At bl = 2048 the alpha stages run as a prime-factor DFT of
-    4095 = 5*7*9*13 (S2DW_PFA=1, the default) instead of an 8192-point
-    Bluestein convolution (S2DW_PFA=0): both are the same transform, so the
-    coefficients of every scale and the synthesised flm agree to rounding
-    (1e-13 relative)."""
+@pytest.mark.parametrize("B,N", [(1024, 4), (2048, 2)])
+def test_prime_factor_alpha_matches_bluestein(B, N, monkeypatch):
+    """At bl = 1024 and bl = 2048 the alpha stages run as prime-factor DFTs
+    (S2DW_PFA=1, the default): 2047 = 23*89 with Rader's algorithm for the
+    length-89 factor, 4095 = 5*7*9*13; S2DW_PFA=0 runs them as Bluestein
+    convolutions of 4096 and 8192 points.  Both are the same transform, so
+    the coefficients of every scale and the synthesised flm agree to
+    rounding (1e-13 relative)."""
     import torch
 
     from s2dw_b200.device import Plan
 
-    B, N, alpha = 2048, 2, 2.0
+    alpha = 2.0
     t = transform_setup(B, N, alpha)
     flm = gaussian_flm(B, seed=5, power=1.2)
     d_flm = torch.from_numpy(np.ascontiguousarray(flm.T)).cuda()
