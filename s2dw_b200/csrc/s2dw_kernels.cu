@@ -242,10 +242,20 @@ __device__ __forceinline__ void lwalk_body(const LwalkArgs &a)
         const int lc = lstart + c * LW_CH;
         const int nl = min(LW_CH, bl - lc);
         if (lc > rampEnd && lc > blo && nl == LW_CH) {
-#pragma unroll 1
+            // every step accumulates, no start value enters: unrolled, so that
+            // the shared-memory reads take constant offsets
+#pragma unroll
             for (int li = 0; li < LW_CH; li += 2) {
                 step(b, li, lc + li, P0{}, false, true);
                 step(b, li + 1, lc + li + 1, P1{}, false, true);
+            }
+        } else if (lc > rampEnd && lc + LW_CH - 1 <= blo && nl == LW_CH) {
+            // a chunk below the scale's l range: the recurrence alone (not the
+            // general path below, whose accumulation would issue predicated off)
+#pragma unroll 1
+            for (int li = 0; li < LW_CH; li += 2) {
+                step(b, li, lc + li, P0{}, false, false);
+                step(b, li + 1, lc + li + 1, P1{}, false, false);
             }
         } else {
 #pragma unroll 1
@@ -1504,6 +1514,54 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 
 // instead of R^2.  About 40 FP64 operations per point against ~240 for the
 // 8192-point Bluestein convolution of the general engine.
 // ===========================================================================
+// Load phase of the prime-factor alpha kernels: the row pair (g, rr) of one
+// transform of odd length N into shared memory, value m at X[pos(m)], with
+// all of a thread's global loads in flight before the first shared store.
+// Analysis: only the rows m < bl = (N+1)/2 are read; the Hermitian completion
+// m >= bl is their conjugate (z(N - m) from the same two values).  Synthesis:
+// the two real rows, z = w(:, b1) + i w(:, b2).
+template <int MODE, int NT, int N, typename Pos>
+__device__ __forceinline__ void pfa_load(const CztArgs &a, double2 *X, Pos pos)
+{
+    constexpr int BL = (N + 1) / 2;
+    const int t = threadIdx.x, g = blockIdx.y, rr = blockIdx.x;
+    if (MODE == CZT_ANA_ALPHA) {
+        constexpr int PB = (BL + NT - 1) / NT;
+        double2 x1[PB], x2[PB];
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            const int m = t + i * NT;
+            if (m < BL) ld_pair(a.in_c + ((size_t)g * BL + m) * (2 * BL) + 2 * rr, x1[i], x2[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            const int m = t + i * NT;
+            if (m < BL) {
+                if (m == 0) { x1[i].y = 0.0; x2[i].y = 0.0; }
+                X[pos(m)] = make_double2(x1[i].x - x2[i].y, x1[i].y + x2[i].x);
+                if (m > 0) X[pos(N - m)] = make_double2(x1[i].x + x2[i].y, x2[i].x - x1[i].y);
+            }
+        }
+    } else {
+        constexpr int PB = (N + NT - 1) / NT;
+        const double *p = a.in_r + (size_t)N * (2 * rr + (size_t)2 * BL * g);
+        double z0[PB], z1[PB];
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            const int m = t + i * NT;
+            if (m < N) {
+                z0[i] = p[m];
+                z1[i] = p[N + m];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            const int m = t + i * NT;
+            if (m < N) X[pos(m)] = make_double2(z0[i], z1[i]);
+        }
+    }
+}
+
 constexpr int PFA_N = 4095, PFA_THREADS = 256;
 
 // cos(2 pi j / R) and sin(2 pi j / R), j < R (local constant tables: with j
@@ -1609,22 +1667,7 @@ __global__ void __launch_bounds__(PFA_THREADS, 3) pfa_alpha_kernel(CztArgs a)
     const int t = threadIdx.x;
     const int bl = a.bl, n = PFA_N;  // n = 2 bl - 1
     const int g = blockIdx.y, rr = blockIdx.x;
-    for (int m = t; m < n; m += PFA_THREADS) {
-        double2 z;
-        if (MODE == CZT_ANA_ALPHA) {  // Hermitian completion in m, as fft_large_kernel
-            const bool lo = m < bl;
-            const double2 *p = a.in_c + ((size_t)g * bl + (lo ? m : n - m)) * (2 * bl) + 2 * rr;
-            double2 x1, x2;
-            ld_pair(p, x1, x2);
-            if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
-            if (m == 0) { x1.y = 0.0; x2.y = 0.0; }
-            z = make_double2(x1.x - x2.y, x1.y + x2.x);
-        } else {  // z = w(:, b1) + i w(:, b2)
-            const double *p = a.in_r + (size_t)m + (size_t)n * (2 * rr + (size_t)2 * bl * g);
-            z = make_double2(p[0], p[n]);
-        }
-        smem[pfa_in_pos(m)] = z;
-    }
+    pfa_load<MODE, PFA_THREADS, PFA_N>(a, smem, [](int m) { return pfa_in_pos(m); });
     __syncthreads();
     pfa_stage<5, 1, SIGN>(smem, t);
     __syncthreads();
@@ -1790,22 +1833,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(
     const int t = threadIdx.x;
     const int bl = a.bl, n = PFB_N;  // n = 2 bl - 1
     const int g = blockIdx.y, rr = blockIdx.x;
-    for (int m = t; m < n; m += NT) {
-        double2 z;
-        if (MODE == CZT_ANA_ALPHA) {
-            const bool lo = m < bl;
-            const double2 *p = a.in_c + ((size_t)g * bl + (lo ? m : n - m)) * (2 * bl) + 2 * rr;
-            double2 x1, x2;
-            ld_pair(p, x1, x2);
-            if (!lo) { x1 = cconj(x1); x2 = cconj(x2); }
-            if (m == 0) { x1.y = 0.0; x2.y = 0.0; }
-            z = make_double2(x1.x - x2.y, x1.y + x2.x);
-        } else {
-            const double *p = a.in_r + (size_t)m + (size_t)n * (2 * rr + (size_t)2 * bl * g);
-            z = make_double2(p[0], p[n]);
-        }
-        X[(m * 15) % 23 + PFB_P * ((m * 31) % 89)] = z;
-    }
+    pfa_load<MODE, NT, PFB_N>(a, X, [](int m) { return (m * 15) % 23 + PFB_P * ((m * 31) % 89); });
     __syncthreads();
     // length-23 DFTs along d1
     for (int d2 = t; d2 < 89; d2 += NT) {
