@@ -1782,7 +1782,7 @@ __device__ __forceinline__ void pfa_dft_out(double2 (&x)[R], double2 *out, int b
 constexpr int PFB_N = 2047;
 constexpr int PFB_P = 25;              // pitch of d2 in the shared row
 constexpr int PFB_XS = PFB_P * 89;     // shared row size
-constexpr int PFB_SP = 98;             // pitch of a Rader column (positions i + 9 j, i < 8, j < 11)
+constexpr int PFB_SP = 103;            // pitch of a Rader column (positions i + 9 j, i < 8, j < 11)
 
 // per position L = i + 8 j of the 88-layout (input digits (q 3) mod 8,
 // (q 7) mod 11): the length-89 index g^-q whose value goes there, and g^q,
@@ -1826,7 +1826,10 @@ __global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(
     extern __shared__ double2 smem[];
     // the row in layout d1 + 25 d2 (pitch 25: conflict-free shared-memory
     // access for the length-23 DFTs, two-way for the output gather); the 23
-    // Rader convolutions in layout i + 9 j (pitch 98 per column)
+    // Rader convolutions in layout i + 9 j (pitch 103 per column: with the
+    // work items (c1, j) taken c1-fastest, the gathers from the row, the
+    // column stores and their reads back are conflict-free but for the
+    // items where j changes)
     double2 *X = smem;
     double2 *Sc = smem + PFB_XS;
     double2 *X0 = Sc + 23 * PFB_SP;
@@ -1846,7 +1849,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(
     // length-89 DFTs along d2 (column c1) by Rader: forward length-8 DFTs of
     // the permuted inputs
     for (int u = t; u < 23 * 11; u += NT) {
-        const int c1 = u / 11, j = u % 11;
+        const int c1 = u % 23, j = u / 23;
         double2 v[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) v[i] = X[c1 + PFB_P * c_rader_src[i + 8 * j]];
@@ -1873,7 +1876,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(
     __syncthreads();
     // inverse length-8 DFTs; y_{g^q} = x_0 + convolution
     for (int u = t; u < 23 * 11; u += NT) {
-        const int c1 = u / 11, j = u % 11;
+        const int c1 = u % 23, j = u / 23;
         double2 v[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) v[i] = Sc[c1 * PFB_SP + i + 9 * j];
