@@ -952,10 +952,39 @@ __global__ void __launch_bounds__(THREADS, (V * THREADS <= 4096 ? 2 : 1)) fft_ke
     const int R0 = (MODE == FFT_ANA_BETA) ? Pi.r(0) : Pf.r(0);
 
     double2 v[V];
+    if (MODE == FFT_SYN_BETA) {
+        // the gamma DFT one sample (row of V) at a time, so that a thread's V
+        // loads of one sample are in flight together (as fft_load, reordered)
+        int src[V];
 #pragma unroll
-    for (int i = 0; i < V; i++) {
-        const int pos = pos_of<V>(i, R0, t, lgM), r = pos >> lgM, k = pos & (M - 1), row = row0 + r;
-        v[i] = (row < a.rows) ? fft_load<MODE>(a, row, k, ph) : make_double2(0.0, 0.0);
+        for (int i = 0; i < V; i++) {
+            const int pos = pos_of<V>(i, R0, t, lgM), row = row0 + (pos >> lgM);
+            src[i] = row < a.rows ? (row % bl) * (2 * bl) + beta_src(pos & (M - 1), bl) : -1;
+            v[i] = make_double2(0.0, 0.0);
+        }
+        for (int gg = 0; gg < N; gg++) {
+            const double2 *Vg = a.in_c + (size_t)gg * bl * (2 * bl);
+#pragma unroll
+            for (int i = 0; i < V; i++) {
+                if (src[i] < 0) continue;
+                const int pos = pos_of<V>(i, R0, t, lgM), q = (row0 + (pos >> lgM)) / bl;
+                v[i] = cadd(v[i], cmul(Vg[src[i]], ph[q * N + gg]));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < V; i++) {
+            if (src[i] < 0) continue;
+            const int pos = pos_of<V>(i, R0, t, lgM), row = row0 + (pos >> lgM), q = row / bl, m = row % bl;
+            const int b = beta_src(pos & (M - 1), bl);
+            const double2 u = cscale(v[i], a.wq[b]);
+            v[i] = (((m + a.nq[q]) & 1) && (b & 1)) ? make_double2(-u.x, -u.y) : u;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < V; i++) {
+            const int pos = pos_of<V>(i, R0, t, lgM), r = pos >> lgM, k = pos & (M - 1), row = row0 + r;
+            v[i] = (row < a.rows) ? fft_load<MODE>(a, row, k, ph) : make_double2(0.0, 0.0);
+        }
     }
 
     int RL;  // radix of the last pass run
@@ -1258,12 +1287,20 @@ __global__ void __launch_bounds__((1 << LGM) / 16, (LGM == 11 ? 4 : LGM == 12 ? 
         // threads), then the DCT-II reordering through shared memory: the
         // value of b goes to FFT index b/2 (b even) or (4bl-1-b)/2 (b odd)
         const bool sn = (rr + a.nq[g]) & 1;
+        // one gamma sample (row of V) at a time: its 16 loads per thread are
+        // independent, so they are all in flight together
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = zero;
+        for (int gg = 0; gg < N; gg++) {
+            const double2 *row = a.in_c + ((size_t)gg * bl + rr) * (2 * bl);
+            const double2 w = ph[gg];
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = cadd(v[i], cmul(row[t + i * THREADS], w));
+        }
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const int b = t + i * THREADS;
-            double2 u = zero;
-            for (int gg = 0; gg < N; gg++) u = cadd(u, cmul(a.in_c[((size_t)gg * bl + rr) * (2 * bl) + b], ph[gg]));
-            u = cscale(u, a.wq[b]);
+            double2 u = cscale(v[i], a.wq[b]);
             if (sn && (b & 1)) u = make_double2(-u.x, -u.y);
             buf[padix((b & 1) ? (4 * bl - 1 - b) >> 1 : b >> 1)] = u;
         }
