@@ -166,6 +166,12 @@ struct MwalkArgs {
     const double2 *V2f;   // [(q*bl + m)*Vs + m']
     int Vs;               // roundup(bl, 8)
     double2 *part;        // this scale's flm contribution [(l-blo-1)*bl + m], m <= l
+    // the same tables transposed for the two-l-per-thread kernel:
+    // GT[(m' (NP+1) + q) Ts + l - blo - 1], q < NP: G; q = NP: b(l, m');
+    // rows m' < roundup(bl, 8), Ts = roundup(bl - blo - 1, 64), zero padded
+    const double *GT;
+    int Ts;
+    int tile_l, tile_m;   // the plan's tile shape (mwalk_tile_l / mwalk_tile_m when it was built)
     const int2 *tiles;    // (l-tile, m-tile) per CTA, longest walks first
     int ntiles;
     // 0: part = result.  1: G holds the second real part b of S = eta (a + i b)
@@ -175,9 +181,16 @@ struct MwalkArgs {
 // Tile lists of the contraction kernels for one scale, ordered by decreasing
 // work so that the longest walks start first.
 void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t);
-void build_mwalk_tiles(int bl, int blo, int wq, std::vector<int2> &t);
+void build_mwalk_tiles(int bl, int blo, int wq, int tl, std::vector<int2> &t);
 int lwalk_tile_m(int NP);  // m values per lwalk CTA tile
 int mwalk_tile_m(int NP);  // m values per mwalk CTA tile
+int mwalk_tile_l(int NP);  // l values per mwalk CTA tile: 64 for the kernel that reads GT, else 32
+struct GsTArgs {
+    int Bp, NP, bl, blo, Gs, Ts, rows;  // rows = roundup(bl, 8)
+    const double *G, *Bcoef;
+    double *out;
+};
+int launch_gsyn_t(const GsTArgs &a, cudaStream_t s);
 
 // flm(l,m) = sum_j part_j(l,m) + Phi2(l) scoeff(l,m), the scale sum of
 // s2dw_core_mod.f90:1228-1253 in scale order followed by :1258-1261.

@@ -592,6 +592,225 @@ __global__ void __launch_bounds__(MW_W * 32, MINB) mwalk_kernel_minb(MwalkArgs a
     mwalk_body<NP, Q>(a);
 }
 
+// ---------------------------------------------------------------------------
+// Synthesis m'-walk with two l per thread (NP <= 4).
+//
+// The broadcast reads of V2f(m, m', q) bound the kernel above: a 16-byte read
+// that every lane takes costs two shared-memory wavefronts, one per (m, q, m')
+// for 32 lanes' worth of FP64 work.  Here each lane walks the pairs of two l
+// (l and l + 32) with QM values of m, so that one broadcast read of V feeds
+// twice the work, and the per-l rows b(l, m') and G(l, m', q) are read per step
+// from a transposed table (GT, l fastest: conflict-free 8-byte reads) instead
+// of being held in registers.  Tile: 64 l x MW_W*QM m; the same chunks of
+// MW_CH m' values, staged by cp.async in a fixed pattern.
+// ---------------------------------------------------------------------------
+constexpr int M2_TL = 64;  // l per tile
+
+template <int NP, int QM>
+struct Mwalk2Smem {
+    static constexpr int WQ = MW_W * QM;
+    static constexpr int R = NP + 1;                               // GT rows per m'
+    static constexpr int T_OFF = 0;                                // double [MW_CH][R][64]
+    static constexpr int V_OFF = T_OFF + MW_CH * R * M2_TL;        // double2 [NP][WQ][MW_CH]
+    static constexpr int BUF = V_OFF + 2 * NP * WQ * MW_CH;
+    static constexpr size_t BYTES = 2 * BUF * sizeof(double);
+};
+
+template <int NP, int QM>
+__device__ __forceinline__ void mwalk2_body(const MwalkArgs &a)
+{
+    using L = Mwalk2Smem<NP, QM>;
+    constexpr int WQ = L::WQ, R = L::R;
+    static_assert(MW_W * 32 == 128 && MW_CH == 8 && (MW_CH * R * M2_TL / 2) % 128 == 0, "staging pattern");
+    extern __shared__ __align__(16) double msm[];
+
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int2 tile = a.tiles[blockIdx.x];
+    const int lt = tile.x, mt = tile.y;
+    const int B = a.B, bl = a.bl, blo = a.blo, Vs = a.Vs, Ts = a.Ts;
+    const int lbase = blo + 1 + lt * M2_TL, mbase = mt * WQ;
+    const int MH = min(lbase + M2_TL - 1, bl - 1);
+    if (mbase > MH) return;  // tile entirely above the diagonal m <= l
+
+    int l[2];
+    double st[2][QM], mq[QM];
+    bool val[2][QM];
+    int maxe = INT_MIN;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        l[i] = lbase + lane + 32 * i;
+#pragma unroll
+        for (int q = 0; q < QM; q++) {
+            const int m = mbase + w * QM + q;
+            val[i][q] = (l[i] < bl) && (m <= l[i]);
+            if (val[i][q]) maxe = max(maxe, (int)a.Ee[(size_t)l[i] * B + m]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < QM; q++) mq[q] = (double)(mbase + w * QM + q);
+    maxe = warp_max_i(maxe);
+    int Kw = (maxe != INT_MIN && maxe < S2DW_SCALE_EXP) ? -maxe : 0;
+    double e[2][QM], ep[2][QM];
+    double2 acc[2][QM];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int q = 0; q < QM; q++) {
+            const int m = mbase + w * QM + q;
+            st[i][q] = 0.0;
+            if (val[i][q]) {
+                const double v = ldexp(a.Em[(size_t)l[i] * B + m], (int)a.Ee[(size_t)l[i] * B + m] + Kw);
+                st[i][q] = ((l[i] - m) & 1) ? -v : v;
+            }
+            e[i][q] = ep[i][q] = 0.0;
+            acc[i][q] = make_double2(0.0, 0.0);
+        }
+
+    const int ctop = MH / MW_CH;  // chunks ctop, ctop-1, ..., 0 cover m' = MH .. 0
+    // V rows of m >= bl are never copied: zeroed once, in both buffers
+    const int nu = min(WQ, bl - mbase);
+    if (nu < WQ)
+        for (int i = tid; i < 2 * L::BUF; i += blockDim.x) {
+            const int r = i % L::BUF;
+            if (r >= L::V_OFF && ((r - L::V_OFF) / (2 * MW_CH)) % WQ >= nu) msm[i] = 0.0;
+        }
+    // GT rows (m', q) of a chunk are consecutive: MW_CH*R rows of 64 doubles
+    // from column lt*64 (16-byte pieces, 32 per row); V2f as in mwalk_kernel
+    const double *gsrc = a.GT + (size_t)lt * M2_TL;
+    auto stage = [&](int c, int buf) {
+        double *b = msm + buf * L::BUF;
+        const double *src = gsrc + (size_t)c * MW_CH * R * Ts;
+#pragma unroll
+        for (int i = 0; i < MW_CH * R * M2_TL / 2 / 128; i++) {
+            const int pc = tid + 128 * i, row = pc >> 5, col = pc & 31;
+            cp16(b + L::T_OFF + row * M2_TL + 2 * col, src + (size_t)row * Ts + 2 * col);
+        }
+        const int c0 = c * MW_CH;
+#pragma unroll
+        for (int i = 0; i < (NP * WQ * MW_CH + 127) / 128; i++) {
+            const int f = tid + 128 * i, kk = f % MW_CH, r = f / MW_CH, u = r % WQ, q = r / WQ;
+            if (f < NP * WQ * MW_CH && mbase + u < bl)
+                cp16(b + L::V_OFF + 2 * (r * MW_CH + kk), a.V2f + ((size_t)q * bl + mbase + u) * Vs + c0 + kk);
+        }
+    };
+
+    stage(ctop, 0);
+    cp_commit();
+    for (int c = ctop, it = 0; c >= 0; c--, it++) {
+        if (c > 0) stage(c - 1, (it + 1) & 1);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        const double *b = msm + (it & 1) * L::BUF;
+        const double *T = b + L::T_OFF;
+        const double2 *Vb = reinterpret_cast<const double2 *>(b + L::V_OFF);
+        const int c0 = c * MW_CH;
+        const bool ramp = (c0 + MW_CH - 1 >= lbase);
+        // one m' step at chunk row k for all pairs (the same operations in the
+        // same order as mwalk_kernel's step)
+        auto mstep = [&](const int k, const bool inj, const int mpv) {
+            double bk[2], gk[2][NP];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                bk[i] = T[(k * R + NP) * M2_TL + lane + 32 * i];
+#pragma unroll
+                for (int kq = 0; kq < NP; kq++) gk[i][kq] = T[(k * R + kq) * M2_TL + lane + 32 * i];
+            }
+#pragma unroll
+            for (int q = 0; q < QM; q++) {
+                double2 v[NP];
+#pragma unroll
+                for (int kq = 0; kq < NP; kq++) v[kq] = Vb[(kq * WQ + w * QM + q) * MW_CH + k];
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    if (inj && mpv == l[i]) e[i][q] = st[i][q];
+                    double zr = 0.0, zi = 0.0;
+#pragma unroll
+                    for (int kq = 0; kq < NP; kq++) {
+                        zr = fma(gk[i][kq], v[kq].x, zr);
+                        zi = fma(gk[i][kq], v[kq].y, zi);
+                    }
+                    acc[i][q].x = fma(e[i][q], zr, acc[i][q].x);
+                    acc[i][q].y = fma(e[i][q], zi, acc[i][q].y);
+                    const double p = mq[q] * bk[i];
+                    const double en = fma(p, e[i][q], -ep[i][q]);
+                    ep[i][q] = e[i][q];
+                    e[i][q] = en;
+                }
+            }
+        };
+        if (!ramp && c0 + MW_CH - 1 <= MH) {
+            // below the tile's l rows: every step runs, no start value enters
+#pragma unroll
+            for (int k = MW_CH - 1; k >= 0; k--) mstep(k, false, 0);
+        } else {
+#pragma unroll 1
+            for (int k = MW_CH - 1; k >= 0; k--) {
+                const int mpv = c0 + k;
+                if (mpv > MH) continue;  // above the top of this tile (warp-uniform)
+                mstep(k, ramp, mpv);
+            }
+        }
+        if (Kw > 0) {
+            double mx = 0.0;
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int q = 0; q < QM; q++) mx = fmax(mx, fmax(fabs(e[i][q]), fabs(ep[i][q])));
+            mx = warp_max(mx);
+            if (mx > ldexp(1.0, S2DW_RENORM_EXP)) {
+                const int Rr = min(S2DW_RENORM_EXP, Kw);
+                const double f = ldexp(1.0, -Rr);
+#pragma unroll
+                for (int i = 0; i < 2; i++)
+#pragma unroll
+                    for (int q = 0; q < QM; q++) {
+                        e[i][q] *= f;
+                        ep[i][q] *= f;
+                        acc[i][q] = cscale(acc[i][q], f);
+                    }
+                Kw -= Rr;
+            }
+        }
+        __syncthreads();
+    }
+    const double sc = ldexp(1.0, -Kw);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int q = 0; q < QM; q++) {
+            if (!val[i][q]) continue;
+            const int m = mbase + w * QM + q;
+            double2 *dst = a.part + (size_t)(l[i] - blo - 1) * bl + m;
+            if (a.acc_imag) *dst = cadd(*dst, cipow(cscale(acc[i][q], sc), m + 1));  // + i * result
+            else *dst = cipow(cscale(acc[i][q], sc), m);
+        }
+}
+
+template <int NP, int QM>
+__global__ void __launch_bounds__(MW_W * 32, 3) mwalk2_kernel(MwalkArgs a)
+{
+    mwalk2_body<NP, QM>(a);
+}
+
+// GT[(m' (NP+1) + q) Ts + l'] from G (q < NP) and b(l, m') (q = NP), l = blo+1+l';
+// zero for l' >= bl-blo-1 or m' >= bl.
+__global__ void gsyn_t_kernel(GsTArgs a)
+{
+    const int nl = a.bl - a.blo - 1, R = a.NP + 1;
+    const long long total = (long long)a.rows * R * a.Ts;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int lp = (int)(i % a.Ts);
+        const long long r = i / a.Ts;
+        const int q = (int)(r % R), x = (int)(r / R);
+        double v = 0.0;
+        if (lp < nl && x < a.bl)
+            v = q < a.NP ? a.G[((size_t)lp * a.NP + q) * a.Gs + x] : a.Bcoef[(size_t)(a.blo + 1 + lp) * a.Bp + x];
+        a.out[i] = v;
+    }
+}
+
 // ===========================================================================
 // Chirp-z transform engine: power-of-two FFTs in shared memory
 // ===========================================================================
@@ -2017,7 +2236,18 @@ static int launch_lwalk_np(const LwalkArgs &a, cudaStream_t s)
 static int g_lwalk_variant = 0, g_mwalk_variant = 0;
 
 int lwalk_tile_m(int NP) { return LW_W * (NP > 4 ? 2 : 4); }  // pairs per thread: 4, or 2 for N > 8
-int mwalk_tile_m(int NP) { return MW_W * (g_mwalk_variant == 1 && NP <= 4 ? 8 : 4); }
+// the two-l-per-thread synthesis kernel (the default, variant 4), for N <= 8
+// (NP <= 4; 4 m per thread for NP <= 2, 2 for NP = 3, 4); measured on B200 at
+// B=1024, N=4: 343 -> 322 us per full-band launch, FP64 pipe 49 -> 61 %,
+// shared-memory wavefronts 61 -> 43 % of peak
+static bool mwalk2_used(int NP) { return g_mwalk_variant == 4 && NP <= 4; }
+static int mwalk2_qm(int NP) { return NP <= 2 ? 4 : 2; }
+int mwalk_tile_m(int NP)
+{
+    if (mwalk2_used(NP)) return MW_W * mwalk2_qm(NP);
+    return MW_W * (g_mwalk_variant == 1 && NP <= 4 ? 8 : 4);
+}
+int mwalk_tile_l(int NP) { return mwalk2_used(NP) ? M2_TL : 32; }
 
 void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t)
 {
@@ -2032,16 +2262,16 @@ void build_lwalk_tiles(int bl, int blo, int ws, std::vector<int2> &t)
     (void)blo;
 }
 
-void build_mwalk_tiles(int bl, int blo, int wq, std::vector<int2> &t)
+void build_mwalk_tiles(int bl, int blo, int wq, int th, std::vector<int2> &t)
 {
-    // tile (lt, mt) covers l in [blo+1+32 lt, +32), m in [wq mt, +wq); its
+    // tile (lt, mt) covers l in [blo+1+th lt, +th), m in [wq mt, +wq); its
     // walk length is ~ the largest l; tiles entirely above m <= l are dropped
     t.clear();
     const int nl = bl - blo - 1;
     if (nl <= 0) return;
-    const int tl = (nl + 31) / 32, tm = (bl + wq - 1) / wq;
+    const int tl = (nl + th - 1) / th, tm = (bl + wq - 1) / wq;
     for (int lt = tl - 1; lt >= 0; lt--) {
-        const int lmax = std::min(blo + 1 + lt * 32 + 31, bl - 1);
+        const int lmax = std::min(blo + 1 + lt * th + th - 1, bl - 1);
         for (int mt = 0; mt < tm; mt++)
             if (mt * wq <= lmax) t.push_back(make_int2(lt, mt));
     }
@@ -2113,6 +2343,36 @@ static int launch_mwalk_np(const MwalkArgs &a, cudaStream_t s)
     return S2DWC_OK;
 }
 
+template <int NP, int QM>
+static int launch_mwalk2(const MwalkArgs &a, cudaStream_t s)
+{
+    using L = Mwalk2Smem<NP, QM>;
+    if (a.bl - a.blo - 1 <= 0 || a.ntiles <= 0) return S2DWC_OK;
+    if (!a.GT) return set_error(S2DWC_ERROR_ARG_INVALID, "mwalk2: transposed tables missing");
+    static bool attr[64] = {false};
+    int dev = 0;
+    S2DW_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        S2DW_CUDA_TRY(cudaFuncSetAttribute(mwalk2_kernel<NP, QM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::BYTES));
+        attr[dev] = true;
+    }
+    mwalk2_kernel<NP, QM><<<a.ntiles, MW_W * 32, L::BYTES, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+int launch_gsyn_t(const GsTArgs &a, cudaStream_t s)
+{
+    const long long total = (long long)a.rows * (a.NP + 1) * a.Ts;
+    if (total <= 0) return S2DWC_OK;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    gsyn_t_kernel<<<(int)blocks, 256, 0, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
 template <int Q, int MINB>
 static int launch_mwalk_q(const MwalkArgs &a, cudaStream_t s)
 {
@@ -2132,8 +2392,20 @@ static int launch_mwalk_q(const MwalkArgs &a, cudaStream_t s)
 
 int launch_mwalk(const MwalkArgs &a, cudaStream_t s)
 {
+    // the kernel follows the plan's tile shape
+    if (a.tile_l == M2_TL) {
+        if (a.NP > 4 || a.tile_m != MW_W * mwalk2_qm(a.NP))
+            return set_error(S2DWC_ERROR_ARG_INVALID, "mwalk: tile shape %dx%d for NP=%d", a.tile_l, a.tile_m, a.NP);
+        switch (a.NP) {
+        case 1: return launch_mwalk2<1, 4>(a, s);
+        case 2: return launch_mwalk2<2, 4>(a, s);
+        case 3: return launch_mwalk2<3, 2>(a, s);
+        default: return launch_mwalk2<4, 2>(a, s);
+        }
+    }
+    if (a.tile_l != 32) return set_error(S2DWC_ERROR_ARG_INVALID, "mwalk: tile height %d", a.tile_l);
+    if (a.tile_m == MW_W * 8) return launch_mwalk_q<8, 0>(a, s);
     switch (g_mwalk_variant) {
-    case 1: return launch_mwalk_q<8, 0>(a, s);
     case 2: return launch_mwalk_q<4, 5>(a, s);
     case 3: return launch_mwalk_q<4, 4>(a, s);
     // 3 CTAs/SM (<= 168 registers, no spills): 3-10 % faster than 4 CTAs/SM

@@ -53,6 +53,14 @@ struct s2dwc_plan {
     double *kappaA_b = nullptr, *kappaS_b = nullptr, *Ga_b = nullptr, *Gsyn_b = nullptr;
     std::vector<long long> ga_off, gs_off;       // per-scale offsets (doubles)
     std::vector<int> ga_stride, gs_stride;
+    // synthesis tables transposed for the two-l-per-thread m'-walk (MwalkArgs::GT),
+    // when the plan's tiles are 64 l high: per scale roundup(bl, 8) x (NP+1) rows
+    // of gt_ld[j] = roundup(bl-blo-1, 64) values
+    int mw_tile_l = 32, mw_tile_m = 16;
+    double *GsT = nullptr, *GsT_b = nullptr;
+    long long gt_total = 0;
+    std::vector<long long> gt_off;
+    std::vector<int> gt_ld;
     double2 *Fw = nullptr;                       // per-call F table [l*Bp + m]
     // per-scale workspaces (scales run concurrently on their own streams):
     // A_j holds Tb / V (N x bl x 2bl), C_j holds Tg (N x bl x bl) / V2f,
@@ -367,6 +375,19 @@ int plan_build(s2dwc_plan *p)
     }
     p->ga_total = na;
     p->gs_total = ns;
+    p->mw_tile_l = mwalk_tile_l(p->NP);
+    p->mw_tile_m = mwalk_tile_m(p->NP);
+    if (p->mw_tile_l == 64) {
+        long long nt = 0;
+        for (int j = 0; j <= J; j++) {
+            const int nl = std::max(0, p->bl[j] - p->blo[j] - 1);
+            p->gt_ld.push_back((nl + 63) / 64 * 64);
+            p->gt_off.push_back(nt);
+            nt += (long long)(p->bl[j] + 7) / 8 * 8 * (p->NP + 1) * p->gt_ld[j];
+        }
+        p->gt_total = nt;
+        if ((st = dev_alloc(p, &p->GsT, (size_t)std::max(1LL, nt)))) return st;
+    }
     if ((st = dev_alloc(p, &p->Ga, (size_t)std::max(1LL, na))) ||
         (st = dev_alloc(p, &p->Gsyn, (size_t)std::max(1LL, ns))) ||
         (st = dev_alloc(p, &p->Fw, (size_t)B * Bp)))
@@ -392,7 +413,7 @@ int plan_build(s2dwc_plan *p)
         if ((st = dev_upload(p, &d, tl))) return st;
         p->lw_tiles.push_back(d);
         p->lw_ntiles.push_back((int)tl.size());
-        build_mwalk_tiles(p->bl[j], p->blo[j], mwalk_tile_m(p->NP), tl);
+        build_mwalk_tiles(p->bl[j], p->blo[j], p->mw_tile_m, p->mw_tile_l, tl);
         d = nullptr;
         if (tl.empty()) tl.push_back(make_int2(0, 0));  // keep a valid allocation
         if ((st = dev_upload(p, &d, tl))) return st;
@@ -644,6 +665,10 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         ma.V2f = V2f;
         ma.Vs = p->gs_stride[j];
         ma.part = p->wsP + p->offP[j];
+        ma.GT = p->GsT ? p->GsT + p->gt_off[j] : nullptr;
+        ma.Ts = p->GsT ? p->gt_ld[j] : 0;
+        ma.tile_l = p->mw_tile_l;
+        ma.tile_m = p->mw_tile_m;
         ma.tiles = p->mw_tiles[j];
         ma.ntiles = p->mw_ntiles[j];
         {
@@ -652,6 +677,7 @@ int run_synthesis(s2dwc_plan *p, double2 *d_flm, const double *d_wav, const doub
         }
         if (p->slm_general) {  // the b part of a general Slm, accumulated into part
             ma.G = p->Gsyn_b + p->gs_off[j];
+            if (p->GsT) ma.GT = p->GsT_b + p->gt_off[j];
             ma.acc_imag = 1;
             KernelTimer kt(p, S2DWC_KIND_MWALK, sj);
             if ((st = launch_mwalk(ma, sj))) return st;
@@ -1225,7 +1251,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
     }
     {
         const char *lw = getenv("S2DW_LWALK_VARIANT"), *mw = getenv("S2DW_MWALK_VARIANT");
-        set_walk_variants(lw ? atoi(lw) : 0, mw ? atoi(mw) : 0);
+        // default synthesis kernel: two l per thread (4; N > 8 falls back to 0)
+        set_walk_variants(lw ? atoi(lw) : 0, mw ? atoi(mw) : 4);
     }
     auto *p = new s2dwc_plan();
     p->B = B;
@@ -1333,7 +1360,8 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
         if ((st = dev_alloc(p, &p->kappaA_b, (size_t)(J + 1) * B * NP)) ||
             (st = dev_alloc(p, &p->kappaS_b, (size_t)(J + 1) * B * NP)) ||
             (st = dev_alloc(p, &p->Ga_b, (size_t)std::max(1LL, p->ga_total))) ||
-            (st = dev_alloc(p, &p->Gsyn_b, (size_t)std::max(1LL, p->gs_total))))
+            (st = dev_alloc(p, &p->Gsyn_b, (size_t)std::max(1LL, p->gs_total))) ||
+            (p->GsT && (st = dev_alloc(p, &p->GsT_b, (size_t)std::max(1LL, p->gt_total)))))
             return st;
     }
     if (general) {
@@ -1380,6 +1408,25 @@ int s2dwc_plan_set_tables(s2dwc_plan *p, const double *K_gamma, const double *Ph
             g.stride = p->gs_stride[j];
             g.out = p->Gsyn_b + p->gs_off[j];
             if ((st = launch_gprep(g, 0))) return st;
+        }
+        if (p->GsT) {
+            GsTArgs t{};
+            t.Bp = p->Bp;
+            t.NP = NP;
+            t.bl = p->bl[j];
+            t.blo = p->blo[j];
+            t.Gs = p->gs_stride[j];
+            t.Ts = p->gt_ld[j];
+            t.rows = (p->bl[j] + 7) / 8 * 8;
+            t.G = p->Gsyn + p->gs_off[j];
+            t.Bcoef = p->Bcoef;
+            t.out = p->GsT + p->gt_off[j];
+            if ((st = launch_gsyn_t(t, 0))) return st;
+            if (general) {
+                t.G = p->Gsyn_b + p->gs_off[j];
+                t.out = p->GsT_b + p->gt_off[j];
+                if ((st = launch_gsyn_t(t, 0))) return st;
+            }
         }
     }
     S2DW_CUDA_TRY(cudaDeviceSynchronize());

@@ -395,3 +395,40 @@ def test_host_api_table_changes_take_effect():
     for a, b in zip(wA, w3):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(scA, sc3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,N,alpha,general", [(64, 3, 2.0, False), (128, 4, 2.0, False), (96, 5, 2.0, False),
+                                               (128, 8, 2.0, False), (64, 4, 2.0, True)])
+def test_mwalk_two_l_kernel_is_bit_identical(B, N, alpha, general, monkeypatch):
+    """The synthesis contraction with two l per thread and transposed tables
+    (S2DW_MWALK_VARIANT=4, the default for N <= 8) does the same operations
+    per (l, m) pair in the same order as the 32-l kernel (variant 0), so the
+    synthesised flm is bit-identical (also for a general complex Slm, whose
+    second pass reads the tables of b)."""
+    import torch
+
+    from s2dw_b200.device import Plan
+
+    t = transform_setup(B, N, alpha)
+    J, bs2 = t["J"], max(1, t["bl_scoeff"] ** 2)
+    Slm = t["Slm"]
+    if general:
+        rng = np.random.default_rng(7)
+        Slm = np.asfortranarray(Slm + 0.3j * rng.standard_normal(Slm.shape) * (np.abs(Slm) > 0))
+    out = {}
+    for v in ("0", "4"):
+        monkeypatch.setenv("S2DW_MWALK_VARIANT", v)
+        p = Plan(B, N, alpha, J)
+        p.set_tables(t["K_gamma"], t["Phi2"], Slm, t["bl_scoeff"])
+        w = torch.from_numpy(np.random.default_rng(B + N).standard_normal(p.wav_size)).cuda()
+        sc = torch.zeros(bs2, dtype=torch.complex128, device="cuda")
+        f = torch.empty((B, B), dtype=torch.complex128, device="cuda")
+        p.synthesis(w, sc, f)
+        torch.cuda.synchronize()
+        out[v] = f.cpu().numpy()
+        p.close()
+    monkeypatch.delenv("S2DW_MWALK_VARIANT")
+    Plan(16, 2, 2.0, core.s2dw_core_comp_Jmax(16, 2.0)).close()  # restore the default for later tests
+    assert np.abs(out["4"]).max() > 0
+    np.testing.assert_array_equal(out["4"], out["0"])
