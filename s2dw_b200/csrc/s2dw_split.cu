@@ -575,21 +575,31 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         const int wmp = p0 + ch;
         Chain cn = chain_init(a.Ste, a.Stm, a.B, m, wmp, walker && wmp < bl);
         double *WT = reinterpret_cast<double *>(sm + S::WT) + warp * 2 * S::WT_DBL;
+        // staging: a fixed pattern per lane (its 16-byte piece of an Ap row,
+        // rows in passes; one row of Am and Om), so that a copy costs a row
+        // bound check and one address computation
+        static_assert(KC == 32 && (WL == 16 || WL == 32), "walker staging pattern");
+        constexpr int V = WL / 2, RP = 32 / V;  // pieces per Ap row, rows per pass
+        const int pc = lane % V, col = p0 + warp * 32 + 2 * pc;
+        const bool colok = col < a.Bp;
         auto stage = [&](int c, int b) {
             double *T = WT + b * S::WT_DBL;
             const int lb = c * KC;
-            constexpr int V = WL / 2;
-            for (int i = lane; i < KC * V; i += 32) {
-                const int li = i / V, x = 2 * (i % V), l = lb + li, col = p0 + warp * 32 + x;
-                double *d = T + S::WT_AP + li * WL + x;
-                if (l < bl && col < a.Bp) cp_async16(d, a.Acoef + (size_t)l * a.Bp + col);
+#pragma unroll
+            for (int k = 0; k < KC / RP; k++) {
+                const int li = lane / V + RP * k, l = lb + li;
+                double *d = T + S::WT_AP + li * WL + 2 * pc;
+                if (l < bl && colok) cp_async16(d, a.Acoef + (size_t)l * a.Bp + col);
                 else { d[0] = 0.0; d[1] = 0.0; }
             }
-            for (int i = lane; i < 2 * KC; i += 32) {
-                const int li = i % KC, l = lb + li;
-                double *d = T + (i < KC ? S::WT_AM : S::WT_OM) + li;
-                if (l < bl) cp_async8(d, (i < KC ? a.Acoef : a.Om) + (size_t)l * a.Bp + m);
-                else *d = 0.0;
+            const int l = lb + lane;
+            double *dm = T + S::WT_AM + lane, *dom = T + S::WT_OM + lane;
+            if (l < bl) {
+                cp_async8(dm, a.Acoef + (size_t)l * a.Bp + m);
+                cp_async8(dom, a.Om + (size_t)l * a.Bp + m);
+            } else {
+                *dm = 0.0;
+                *dom = 0.0;
             }
         };
         if (has_mma) {
@@ -647,15 +657,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) split_kernel(SplitArgs a)
         const int Ed = prow ? (int)a.dexp[((size_t)m * bl + pmp) * NP + pq] : E_ZERO;
         const double dfac = digit_factor(Ed);
         double *GT = reinterpret_cast<double *>(sm + S::GT);
+        // staging: the cutter threads are a whole number of G row groups
+        // (NP rows of CH doubles per l), so each thread copies a fixed piece
+        // (q, x) of every RS-th l
+        constexpr int V = CH / 2, RW = NP * V, RS = NCT / RW;
+        static_assert(NCT % RW == 0, "cutter staging pattern");
+        const int sq = (ct % RW) / V, sx = 2 * ((ct % RW) % V), li0 = ct / RW;
+        const bool sxok = p0 + sx < a.Gs;
         auto stage = [&](int c, int b) {
             double *T = GT + b * S::GT_DBL;
             const int lb = c * KC;
-            constexpr int V = CH / 2;
-            for (int i = ct; i < KC * NP * V; i += NCT) {
-                const int li = i / (NP * V), r = i % (NP * V), q = r / V, x = 2 * (r % V), l = lb + li;
-                double *d = T + (li * NP + q) * CH + x;
-                if (l < bl && l > blo && p0 + x < a.Gs)
-                    cp_async16(d, a.G + ((size_t)(l - blo - 1) * NP + q) * a.Gs + p0 + x);
+            for (int li = li0; li < KC; li += RS) {
+                const int l = lb + li;
+                double *d = T + (li * NP + sq) * CH + sx;
+                if (l < bl && l > blo && sxok)
+                    cp_async16(d, a.G + ((size_t)(l - blo - 1) * NP + sq) * a.Gs + p0 + sx);
                 else { d[0] = 0.0; d[1] = 0.0; }
             }
         };
