@@ -237,6 +237,7 @@ void set_fft_values(int v);  // FFT engine variant: 8 or 16 values per thread, 0
 void set_large_2048(bool on);  // M = 2048 transforms on the one-row-per-CTA engines (default on)
 void set_pfa(bool on);  // prime-factor alpha stages at bl = 2048 and 1024 (default on)
 void set_pfa2047_threads(int n);  // threads per CTA of the length-2047 kernel (128 or 256)
+void set_pfa1023(bool on);         // prime-factor alpha stages at bl = 512
 // Builds, once per device, the constant table of the length-2047 alpha stages
 // (the current device; synchronises).  Plan creation calls it, never a capture.
 int pfa_prepare();

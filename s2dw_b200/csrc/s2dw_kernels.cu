@@ -2162,6 +2162,115 @@ __global__ void __launch_bounds__(NT, (NT == 128 ? 3 : 2)) pfa2047_alpha_kernel(
     }
 }
 
+template <>
+__device__ __forceinline__ void pfa_cs<3>(int j, double &c, double &s)
+{
+    constexpr double C[3] = {
+        1.00000000000000000000, -0.500000000000000000000, -0.500000000000000000000};
+    constexpr double S[3] = {
+        0.0, 0.866025403784438646764, -0.866025403784438646764};
+    c = C[j];
+    s = S[j];
+}
+template <>
+__device__ __forceinline__ void pfa_cs<31>(int j, double &c, double &s)
+{
+    constexpr double C[31] = {
+        1.00000000000000000000, 0.979529941252494493938, 0.918957811620230629127, 0.820763441207276326364,
+        0.688966919075686567801, 0.528964010326962457365, 0.347305252844820285542, 0.151427777504576663657,
+        -0.050649168838712712279, -0.250652532258720539315, -0.440394151557634309516,
+        -0.612105982547662844147, -0.758758122692790901913, -0.874346616144582118827,
+        -0.954139256400048851476, -0.994869323391895146321, -0.994869323391895146321,
+        -0.954139256400048851476, -0.874346616144582118827, -0.758758122692790901913,
+        -0.612105982547662844147, -0.440394151557634309516, -0.250652532258720539315,
+        -0.050649168838712712279, 0.151427777504576663657, 0.347305252844820285542, 0.528964010326962457365,
+        0.688966919075686567801, 0.820763441207276326364, 0.918957811620230629127, 0.979529941252494493938};
+    constexpr double S[31] = {
+        0.0, 0.201298520088660079142, 0.394355855113318580102, 0.571268215094792279157,
+        0.724792787229119958865, 0.848644257494750950464, 0.937752132147080458429, 0.988468324328111399162,
+        0.998716507171052807146, 0.968077118866204305153, 0.897804539570741657137, 0.790775736937698582078,
+        0.651372482722222207454, 0.485301962531081025215, 0.299363122973357954008, 0.101168321987432177786,
+        -0.101168321987432177786, -0.299363122973357954008, -0.485301962531081025215,
+        -0.651372482722222207454, -0.790775736937698582078, -0.897804539570741657137,
+        -0.968077118866204305153, -0.998716507171052807146, -0.988468324328111399162,
+        -0.937752132147080458429, -0.848644257494750950464, -0.724792787229119958865,
+        -0.571268215094792279157, -0.394355855113318580102, -0.201298520088660079142};
+    c = C[j];
+    s = S[j];
+}
+
+// ---------------------------------------------------------------------------
+// Prime-factor alpha stages at bl = 512: n = 1023 = 3 * 11 * 31
+//
+// Good-Thomas as at bl = 2048 (layout L = d1 + 3 d2 + 33 d3, input digits
+// (n u_i) mod R_i with u_i = (1023/R_i)^-1 mod R_i = 2, 9, 16, output k at
+// digits k mod R_i), DFTs of length 3 and 11 in place, then the length-31 DFTs
+// written straight to their output positions (pfa_dft_out keeps their
+// registers to about 31 complex values).  About 45 FP64 operations per point
+// against ~220 for the 2048-point Bluestein convolution.
+// ---------------------------------------------------------------------------
+constexpr int PFC_N = 1023, PFC_THREADS = 128;
+
+__device__ __forceinline__ int pfc_in_pos(int n) { return (n * 2) % 3 + 3 * ((n * 9) % 11) + 33 * ((n * 16) % 31); }
+__device__ __forceinline__ int pfc_out_pos(int k) { return k % 3 + 3 * (k % 11) + 33 * (k % 31); }
+
+// in-place DFTs of length R along stride S of the 1023-point layout
+template <int R, int S, int SIGN>
+__device__ __forceinline__ void pfc_stage(double2 *sm, int t)
+{
+    for (int d = t; d < PFC_N / R; d += PFC_THREADS) {
+        const int base = (d % S) + (d / S) * (S * R);
+        double2 x[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) x[r] = sm[base + r * S];
+        pfa_dft<R, SIGN>(x);
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[base + r * S] = x[r];
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(PFC_THREADS, 3) pfa1023_alpha_kernel(CztArgs a)
+{
+    static_assert(MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA, "alpha stages only");
+    constexpr int SIGN = MODE == CZT_ANA_ALPHA ? +1 : -1;
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = PFC_N;  // n = 2 bl - 1
+    const int g = blockIdx.y, rr = blockIdx.x;
+    pfa_load<MODE, PFC_THREADS, PFC_N>(a, smem, [](int m) { return pfc_in_pos(m); });
+    __syncthreads();
+    pfc_stage<3, 1, SIGN>(smem, t);
+    __syncthreads();
+    pfc_stage<11, 3, SIGN>(smem, t);
+    __syncthreads();
+    // length-31 DFTs along d3 (stride 33), in registers, back to the same positions
+    for (int d = t; d < 33; d += PFC_THREADS) {
+        double2 x[31];
+#pragma unroll
+        for (int r = 0; r < 31; r++) x[r] = smem[d + 33 * r];
+        pfa_dft_out<31, SIGN>(x, smem, d, 33);
+    }
+    __syncthreads();
+    if (MODE == CZT_ANA_ALPHA) {
+        for (int k = t; k < n; k += PFC_THREADS) {
+            const double2 y = smem[pfc_out_pos(k)];
+            double *p = a.out_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            p[0] = y.x;
+            p[n] = y.y;
+        }
+    } else {
+        const double hh = 0.5 * a.scale;
+        for (int m = t; m < bl; m += PFC_THREADS) {
+            const double2 Z = smem[pfc_out_pos(m)];
+            const double2 Zc = cconj(smem[pfc_out_pos(m == 0 ? 0 : n - m)]);
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+}
+
 // ===========================================================================
 // Small kernels
 // ===========================================================================
@@ -2506,6 +2615,16 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
 }
 
 template <int MODE>
+static int launch_pfa1023(const CztArgs &a, cudaStream_t s)
+{
+    const size_t smem = sizeof(double2) * PFC_N;  // 16 KB: no opt-in needed
+    const dim3 grid(a.bl, a.rows / a.bl);          // (b pair, g)
+    pfa1023_alpha_kernel<MODE><<<grid, PFC_THREADS, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+template <int MODE>
 static int launch_pfa(const CztArgs &a, cudaStream_t s)
 {
     const size_t smem = sizeof(double2) * PFA_N;
@@ -2556,7 +2675,9 @@ int pfa_prepare()
     return S2DWC_OK;
 }
 
-static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048 and 1024
+static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048, 1024 and 512
+static bool g_pfa1023 = true;  // bl = 512 (measurement switch)
+void set_pfa1023(bool on) { g_pfa1023 = on; }
 static int g_pfa2047_threads = 128;
 void set_pfa(bool on) { g_pfa = on; }
 void set_pfa2047_threads(int n) { g_pfa2047_threads = n == 256 ? 256 : 128; }
@@ -2599,6 +2720,10 @@ void set_alpha_prefetch(bool on) { g_alpha_prefetch = on; }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
+    if (g_pfa && g_pfa1023 && a.bl == 512 && 2 * a.bl - 1 == PFC_N && a.rows % a.bl == 0) {
+        if (a.mode == CZT_ANA_ALPHA) return launch_pfa1023<CZT_ANA_ALPHA>(a, s);
+        if (a.mode == CZT_SYN_ALPHA) return launch_pfa1023<CZT_SYN_ALPHA>(a, s);
+    }
     if (g_pfa && a.bl == 2048 && 2 * a.bl - 1 == PFA_N && a.rows % a.bl == 0) {
         if (a.mode == CZT_ANA_ALPHA) return launch_pfa<CZT_ANA_ALPHA>(a, s);
         if (a.mode == CZT_SYN_ALPHA) return launch_pfa<CZT_SYN_ALPHA>(a, s);

@@ -1244,6 +1244,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         set_pfa(pf ? atoi(pf) != 0 : true);
         const char *pt = getenv("S2DW_PFA2047_THREADS");
         set_pfa2047_threads(pt ? atoi(pt) : 128);
+        const char *p3 = getenv("S2DW_PFA1023");
+        set_pfa1023(p3 ? atoi(p3) != 0 : true);
     }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");
