@@ -2200,6 +2200,134 @@ __device__ __forceinline__ void pfa_cs<31>(int j, double &c, double &s)
 }
 
 // ---------------------------------------------------------------------------
+// Prime-factor alpha stages at bl = 256: n = 511 = 7 * 73
+//
+// As at bl = 1024 with 23 x 89 replaced by 7 x 73: row layout d1 + 9 d2 (input
+// digits (5n) mod 7, (21n) mod 73), length-7 DFTs along d1, and the length-73
+// DFTs by Rader's algorithm with the primitive root 5: a cyclic convolution of
+// length 72 = 8 x 9 (radix 8 in registers, then length 9; layout L = i + 8 j
+// with input digits q mod 8, (8q) mod 9), the product with the DFT of
+// w_j = exp(SIGN 2 pi i 5^j / 73) (g_rader73_w, built with the length-89 table
+// by pfa_prepare), and the inverse.
+// ---------------------------------------------------------------------------
+constexpr int PFD_N = 511;
+constexpr int PFD_P = 9;               // pitch of d2 in the shared row
+constexpr int PFD_XS = PFD_P * 73;
+constexpr int PFD_SP = 83;             // pitch of a Rader column (positions i + 9 j, i < 8, j < 9)
+constexpr int PFD_THREADS = 128;
+
+__constant__ int c_rader73_src[72] = {
+    1, 22, 46, 63, 72, 51, 27, 10, 37, 11, 23, 68, 36, 62, 50, 5, 55, 42, 48, 34, 18, 31, 25, 39, 64, 21, 24, 17,
+    9, 52, 49, 56, 32, 47, 12, 45, 41, 26, 61, 28, 16, 60, 6, 59, 57, 13, 67, 14, 8, 30, 3, 66, 65, 43, 70, 7, 4,
+    15, 38, 33, 69, 58, 35, 40, 2, 44, 19, 53, 71, 29, 54, 20};
+__constant__ int c_rader73_dst[72] = {
+    1, 10, 27, 51, 72, 63, 46, 22, 2, 20, 54, 29, 71, 53, 19, 44, 4, 40, 35, 58, 69, 33, 38, 15, 8, 7, 70, 43, 65,
+    66, 3, 30, 16, 14, 67, 13, 57, 59, 6, 60, 32, 28, 61, 26, 41, 45, 12, 47, 64, 56, 49, 52, 9, 17, 24, 21, 55,
+    39, 25, 31, 18, 34, 48, 42, 37, 5, 50, 62, 36, 68, 23, 11};
+// [0]: SIGN -1, [1]: SIGN +1; entry k mod 8 + 8 (k mod 9) holds
+// (1/72) sum_j w_j exp(-2 pi i j k / 72)
+__device__ double2 g_rader73_w[2][72];
+
+__global__ void rader73_init_kernel()
+{
+    const int sgn = blockIdx.x ? 1 : -1, k = threadIdx.x;
+    if (k >= 72) return;
+    double re = 0.0, im = 0.0;
+    int gj = 1;  // 5^j mod 73
+    for (int j = 0; j < 72; j++) {
+        double s1, c1, s2, c2;
+        sincospi(2.0 * sgn * gj / 73.0, &s1, &c1);
+        sincospi(-2.0 * ((j * k) % 72) / 72.0, &s2, &c2);
+        re += c1 * c2 - s1 * s2;
+        im += c1 * s2 + s1 * c2;
+        gj = (gj * 5) % 73;
+    }
+    g_rader73_w[blockIdx.x][k % 8 + 8 * (k % 9)] = make_double2(re / 72.0, im / 72.0);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(PFD_THREADS) pfa511_alpha_kernel(CztArgs a)
+{
+    static_assert(MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA, "alpha stages only");
+    constexpr int SIGN = MODE == CZT_ANA_ALPHA ? +1 : -1;
+    constexpr int NT = PFD_THREADS;
+    extern __shared__ double2 smem[];
+    double2 *X = smem;
+    double2 *Sc = smem + PFD_XS;
+    double2 *X0 = Sc + 7 * PFD_SP;
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = PFD_N;  // n = 2 bl - 1
+    const int g = blockIdx.y, rr = blockIdx.x;
+    pfa_load<MODE, NT, PFD_N>(a, X, [](int m) { return (m * 5) % 7 + PFD_P * ((m * 21) % 73); });
+    __syncthreads();
+    // length-7 DFTs along d1
+    for (int d2 = t; d2 < 73; d2 += NT) {
+        double2 x[7];
+#pragma unroll
+        for (int r = 0; r < 7; r++) x[r] = X[PFD_P * d2 + r];
+        pfa_dft_out<7, SIGN>(x, X, PFD_P * d2, 1);
+    }
+    __syncthreads();
+    // length-73 DFTs along d2 (column c1) by Rader: forward length-8 DFTs
+    for (int u = t; u < 7 * 9; u += NT) {
+        const int c1 = u % 7, j = u / 7;
+        double2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = X[c1 + PFD_P * c_rader73_src[i + 8 * j]];
+        Dft<8, -1>::run(v);
+#pragma unroll
+        for (int i = 0; i < 8; i++) Sc[c1 * PFD_SP + i + 9 * j] = v[i];
+        if (j == 0) X0[c1] = X[c1];
+    }
+    __syncthreads();
+    // forward length-9 DFTs, product with the DFT of w, inverse length-9
+    for (int u = t; u < 7 * 8; u += NT) {
+        const int c1 = u / 8, i = u % 8;
+        double2 v[9];
+#pragma unroll
+        for (int jj = 0; jj < 9; jj++) v[jj] = Sc[c1 * PFD_SP + i + 9 * jj];
+        pfa_dft<9, -1>(v);
+        if (i == 0) X[c1] = cadd(X0[c1], v[0]);  // y_0 = x_0 + sum of the other inputs
+#pragma unroll
+        for (int kk = 0; kk < 9; kk++) v[kk] = cmul(v[kk], g_rader73_w[SIGN > 0 ? 1 : 0][i + 8 * kk]);
+        pfa_dft<9, +1>(v);
+#pragma unroll
+        for (int jj = 0; jj < 9; jj++) Sc[c1 * PFD_SP + i + 9 * jj] = v[jj];
+    }
+    __syncthreads();
+    // inverse length-8 DFTs; y_{g^q} = x_0 + convolution
+    for (int u = t; u < 7 * 9; u += NT) {
+        const int c1 = u % 7, j = u / 7;
+        double2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = Sc[c1 * PFD_SP + i + 9 * j];
+        Dft<8, +1>::run(v);
+        const double2 x0 = X0[c1];
+#pragma unroll
+        for (int i = 0; i < 8; i++) X[c1 + PFD_P * c_rader73_dst[i + 8 * j]] = cadd(x0, v[i]);
+    }
+    __syncthreads();
+    if (MODE == CZT_ANA_ALPHA) {
+        for (int k = t; k < n; k += NT) {
+            const double2 y = X[k % 7 + PFD_P * (k % 73)];
+            double *p = a.out_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            p[0] = y.x;
+            p[n] = y.y;
+        }
+    } else {
+        const double hh = 0.5 * a.scale;
+        for (int m = t; m < bl; m += NT) {
+            const int mc = m == 0 ? 0 : n - m;
+            const double2 Z = X[m % 7 + PFD_P * (m % 73)];
+            const double2 Zc = cconj(X[mc % 7 + PFD_P * (mc % 73)]);
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Prime-factor alpha stages at bl = 512: n = 1023 = 3 * 11 * 31
 //
 // Good-Thomas as at bl = 2048 (layout L = d1 + 3 d2 + 33 d3, input digits
@@ -2615,6 +2743,16 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
 }
 
 template <int MODE>
+static int launch_pfa511(const CztArgs &a, cudaStream_t s)
+{
+    const size_t smem = sizeof(double2) * (PFD_XS + 7 * PFD_SP + 7);  // 20 KB: no opt-in needed
+    const dim3 grid(a.bl, a.rows / a.bl);                              // (b pair, g)
+    pfa511_alpha_kernel<MODE><<<grid, PFD_THREADS, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+
+template <int MODE>
 static int launch_pfa1023(const CztArgs &a, cudaStream_t s)
 {
     const size_t smem = sizeof(double2) * PFC_N;  // 16 KB: no opt-in needed
@@ -2670,14 +2808,18 @@ int pfa_prepare()
     if (g_rader_ready[dev]) return S2DWC_OK;
     rader_init_kernel<<<2, 96>>>();
     S2DW_CUDA_TRY(cudaGetLastError());
+    rader73_init_kernel<<<2, 96>>>();
+    S2DW_CUDA_TRY(cudaGetLastError());
     S2DW_CUDA_TRY(cudaStreamSynchronize(0));
     g_rader_ready[dev] = true;
     return S2DWC_OK;
 }
 
-static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048, 1024 and 512
+static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048, 1024, 512 and 256
 static bool g_pfa1023 = true;  // bl = 512 (measurement switch)
+static bool g_pfa511 = true;   // bl = 256 (measurement switch)
 void set_pfa1023(bool on) { g_pfa1023 = on; }
+void set_pfa511(bool on) { g_pfa511 = on; }
 static int g_pfa2047_threads = 128;
 void set_pfa(bool on) { g_pfa = on; }
 void set_pfa2047_threads(int n) { g_pfa2047_threads = n == 256 ? 256 : 128; }
@@ -2720,6 +2862,14 @@ void set_alpha_prefetch(bool on) { g_alpha_prefetch = on; }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
+    if (g_pfa && g_pfa511 && a.bl == 256 && 2 * a.bl - 1 == PFD_N && a.rows % a.bl == 0) {
+        int dev = 0;
+        S2DW_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64 || !g_rader_ready[dev])
+            return set_error(S2DWC_ERROR_NOT_INIT, "the length-511 alpha tables are not built on device %d", dev);
+        if (a.mode == CZT_ANA_ALPHA) return launch_pfa511<CZT_ANA_ALPHA>(a, s);
+        if (a.mode == CZT_SYN_ALPHA) return launch_pfa511<CZT_SYN_ALPHA>(a, s);
+    }
     if (g_pfa && g_pfa1023 && a.bl == 512 && 2 * a.bl - 1 == PFC_N && a.rows % a.bl == 0) {
         if (a.mode == CZT_ANA_ALPHA) return launch_pfa1023<CZT_ANA_ALPHA>(a, s);
         if (a.mode == CZT_SYN_ALPHA) return launch_pfa1023<CZT_SYN_ALPHA>(a, s);

@@ -421,7 +421,10 @@ int plan_build(s2dwc_plan *p)
         p->mw_ntiles.push_back(p->bl[j] - p->blo[j] - 1 > 0 ? (int)tl.size() : 0);
     }
     if (p->dry) return S2DWC_OK;
-    if (std::find(p->bl.begin(), p->bl.end(), 1024) != p->bl.end() && (st = pfa_prepare())) return st;
+    if ((std::find(p->bl.begin(), p->bl.end(), 1024) != p->bl.end() ||
+         std::find(p->bl.begin(), p->bl.end(), 256) != p->bl.end()) &&
+        (st = pfa_prepare()))
+        return st;
     p->streams.resize(J + 1);
     p->ev_join.resize(J + 1);
     for (int j = 0; j <= J; j++) {
@@ -1246,6 +1249,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         set_pfa2047_threads(pt ? atoi(pt) : 128);
         const char *p3 = getenv("S2DW_PFA1023");
         set_pfa1023(p3 ? atoi(p3) != 0 : true);
+        const char *p5 = getenv("S2DW_PFA511");
+        set_pfa511(p5 ? atoi(p5) != 0 : true);
     }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");

@@ -133,11 +133,11 @@ def test_alpha_prefetch_kernel_identical(B, N, alpha, monkeypatch):
 @pytest.mark.gpu
 @pytest.mark.parametrize("B,N", [(1024, 4), (2048, 2)])
 def test_prime_factor_alpha_matches_bluestein(B, N, monkeypatch):
-    """At bl = 512, 1024 and 2048 the alpha stages run as prime-factor DFTs
-    (S2DW_PFA=1, the default): 1023 = 3*11*31, 2047 = 23*89 with Rader's
-    algorithm for the length-89 factor, 4095 = 5*7*9*13; S2DW_PFA=0 runs them
-    as Bluestein convolutions of 2048, 4096 and 8192 points (B=1024 has
-    scales with bl = 512 and 1024, B=2048 with bl = 512, 1024 and 2048).  Both are the same transform, so
+    """At bl = 256, 512, 1024 and 2048 the alpha stages run as prime-factor
+    DFTs (S2DW_PFA=1, the default): 511 = 7*73 and 2047 = 23*89 with Rader's
+    algorithm for the prime factor, 1023 = 3*11*31, 4095 = 5*7*9*13;
+    S2DW_PFA=0 runs them as Bluestein convolutions of 1024 to 8192 points
+    (B=1024 has scales with bl = 256, 512 and 1024, B=2048 also 2048).  Both are the same transform, so
     the coefficients of every scale and the synthesised flm agree to
     rounding (1e-13 relative)."""
     import torch
