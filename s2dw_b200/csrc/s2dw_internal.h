@@ -239,6 +239,7 @@ void set_pfa(bool on);  // prime-factor alpha stages at bl = 2048 and 1024 (defa
 void set_pfa2047_threads(int n);  // threads per CTA of the length-2047 kernel (128 or 256)
 void set_pfa1023(bool on);         // prime-factor alpha stages at bl = 512
 void set_pfa511(bool on);          // prime-factor alpha stages at bl = 256
+void set_pfa_small(bool on);       // prime-factor alpha stages at bl = 2, 4, 8, 16, 32, 128
 // Builds, once per device, the constant table of the length-2047 alpha stages
 // (the current device; synchronises).  Plan creation calls it, never a capture.
 int pfa_prepare();

@@ -2399,6 +2399,99 @@ __global__ void __launch_bounds__(PFC_THREADS, 3) pfa1023_alpha_kernel(CztArgs a
     }
 }
 
+template <>
+__device__ __forceinline__ void pfa_cs<17>(int j, double &c, double &s)
+{
+    constexpr double C[17] = {
+        1.00000000000000000000, 0.932472229404355804573, 0.739008917220659115925, 0.445738355776538267396,
+        0.092268359463301995240, -0.273662990072082863539, -0.602634636379256389179, -0.850217135729614152134,
+        -0.982973099683901778282, -0.982973099683901778282, -0.850217135729614152134, -0.602634636379256389179,
+        -0.273662990072082863539, 0.092268359463301995240, 0.445738355776538267396, 0.739008917220659115925,
+        0.932472229404355804573};
+    constexpr double S[17] = {
+        0.0, 0.361241666187152948745, 0.673695643646557211713, 0.895163291355062322067, 0.995734176295034521871,
+        0.961825643172819070409, 0.798017227280239503333, 0.526432162877355800245, 0.183749517816570331574,
+        -0.183749517816570331574, -0.526432162877355800245, -0.798017227280239503333, -0.961825643172819070409,
+        -0.995734176295034521871, -0.895163291355062322067, -0.673695643646557211713, -0.361241666187152948745};
+    c = C[j];
+    s = S[j];
+}
+
+// ---------------------------------------------------------------------------
+// Prime-factor alpha stages of the small scales: n = 2bl - 1 = R1 R2 R3 with
+// small pairwise coprime factors (bl = 2: 3; 4: 7; 8: 3 * 5; 16: 31; 32: 7 * 9;
+// 128: 3 * 5 * 17), Good-Thomas with direct symmetric-pair DFTs (factors of 1
+// are skipped), one CTA per row pair as the kernels above.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int pfs_inv(int a, int r)
+{
+    int x = 1;
+    while (r > 1 && (a * x) % r != 1) x++;
+    return x;
+}
+
+template <int N, int R, int S>
+__device__ __forceinline__ void pfs_stage(double2 *sm, int t, int nt, int sign)
+{
+    for (int d = t; d < N / R; d += nt) {
+        const int base = (d % S) + (d / S) * (S * R);
+        double2 x[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) x[r] = sm[base + r * S];
+        if (sign > 0) pfa_dft<R, +1>(x);
+        else pfa_dft<R, -1>(x);
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[base + r * S] = x[r];
+    }
+}
+
+constexpr int PFS_THREADS = 64;
+
+template <int R1, int R2, int R3, int MODE>
+__global__ void __launch_bounds__(PFS_THREADS) pfs_alpha_kernel(CztArgs a)
+{
+    static_assert(MODE == CZT_ANA_ALPHA || MODE == CZT_SYN_ALPHA, "alpha stages only");
+    constexpr int SIGN = MODE == CZT_ANA_ALPHA ? +1 : -1;
+    constexpr int N = R1 * R2 * R3, NT = PFS_THREADS;
+    constexpr int U1 = pfs_inv((N / R1) % R1, R1), U2 = pfs_inv((N / R2) % R2, R2), U3 = pfs_inv((N / R3) % R3, R3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x;
+    const int bl = a.bl, n = N;  // n = 2 bl - 1
+    const int g = blockIdx.y, rr = blockIdx.x;
+    pfa_load<MODE, NT, N>(a, smem, [](int m) {
+        return (m * U1) % R1 + R1 * ((m * U2) % R2) + R1 * R2 * ((m * U3) % R3);
+    });
+    __syncthreads();
+    if constexpr (R1 > 1) pfs_stage<N, R1, 1>(smem, t, NT, SIGN);
+    __syncthreads();
+    if constexpr (R2 > 1) {
+        pfs_stage<N, R2, R1>(smem, t, NT, SIGN);
+        __syncthreads();
+    }
+    if constexpr (R3 > 1) {
+        pfs_stage<N, R3, R1 * R2>(smem, t, NT, SIGN);
+        __syncthreads();
+    }
+    auto opos = [](int k) { return k % R1 + R1 * (k % R2) + R1 * R2 * (k % R3); };
+    if (MODE == CZT_ANA_ALPHA) {
+        for (int k = t; k < n; k += NT) {
+            const double2 y = smem[opos(k)];
+            double *p = a.out_r + (size_t)k + (size_t)n * (2 * rr + (size_t)2 * bl * g);
+            p[0] = y.x;
+            p[n] = y.y;
+        }
+    } else {
+        const double hh = 0.5 * a.scale;
+        for (int m = t; m < bl; m += NT) {
+            const double2 Z = smem[opos(m)];
+            const double2 Zc = cconj(smem[opos(m == 0 ? 0 : n - m)]);
+            const double2 sm = cadd(Z, Zc), d = csub(Z, Zc);
+            st_pair(a.out_c + ((size_t)g * bl + m) * (2 * bl) + 2 * rr, make_double2(sm.x * hh, sm.y * hh),
+                    make_double2(d.y * hh, -d.x * hh));
+        }
+    }
+}
+
 // ===========================================================================
 // Small kernels
 // ===========================================================================
@@ -2742,6 +2835,22 @@ static int launch_large(const CztArgs &a, cudaStream_t s)
     return set_error(S2DWC_ERROR_ARG_INVALID, "unknown transform mode %d", a.mode);
 }
 
+template <int R1, int R2, int R3, int MODE>
+static int launch_pfs(const CztArgs &a, cudaStream_t s)
+{
+    const size_t smem = sizeof(double2) * (R1 * R2 * R3);
+    const dim3 grid(a.bl, a.rows / a.bl);  // (b pair, g)
+    pfs_alpha_kernel<R1, R2, R3, MODE><<<grid, PFS_THREADS, smem, s>>>(a);
+    S2DW_CUDA_TRY(cudaGetLastError());
+    return S2DWC_OK;
+}
+template <int R1, int R2, int R3>
+static int launch_pfs_m(const CztArgs &a, cudaStream_t s)
+{
+    return a.mode == CZT_ANA_ALPHA ? launch_pfs<R1, R2, R3, CZT_ANA_ALPHA>(a, s)
+                                   : launch_pfs<R1, R2, R3, CZT_SYN_ALPHA>(a, s);
+}
+
 template <int MODE>
 static int launch_pfa511(const CztArgs &a, cudaStream_t s)
 {
@@ -2818,6 +2927,8 @@ int pfa_prepare()
 static bool g_pfa = true;  // prime-factor alpha stages at bl = 2048, 1024, 512 and 256
 static bool g_pfa1023 = true;  // bl = 512 (measurement switch)
 static bool g_pfa511 = true;   // bl = 256 (measurement switch)
+static bool g_pfa_small = true;  // bl = 2 .. 128 except 64 (measurement switch)
+void set_pfa_small(bool on) { g_pfa_small = on; }
 void set_pfa1023(bool on) { g_pfa1023 = on; }
 void set_pfa511(bool on) { g_pfa511 = on; }
 static int g_pfa2047_threads = 128;
@@ -2862,6 +2973,17 @@ void set_alpha_prefetch(bool on) { g_alpha_prefetch = on; }
 
 int launch_czt(const CztArgs &a, cudaStream_t s)
 {
+    if (g_pfa && g_pfa_small && (a.mode == CZT_ANA_ALPHA || a.mode == CZT_SYN_ALPHA) && a.rows % a.bl == 0) {
+        switch (a.bl) {
+        case 2: return launch_pfs_m<3, 1, 1>(a, s);
+        case 4: return launch_pfs_m<7, 1, 1>(a, s);
+        case 8: return launch_pfs_m<3, 5, 1>(a, s);
+        case 16: return launch_pfs_m<31, 1, 1>(a, s);
+        case 32: return launch_pfs_m<7, 9, 1>(a, s);
+        case 128: return launch_pfs_m<3, 5, 17>(a, s);
+        default: break;
+        }
+    }
     if (g_pfa && g_pfa511 && a.bl == 256 && 2 * a.bl - 1 == PFD_N && a.rows % a.bl == 0) {
         int dev = 0;
         S2DW_CUDA_TRY(cudaGetDevice(&dev));

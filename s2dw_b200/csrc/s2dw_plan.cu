@@ -1251,6 +1251,8 @@ int s2dwc_plan_create(s2dwc_plan **plan, int B, int N, double alpha, int J, int 
         set_pfa1023(p3 ? atoi(p3) != 0 : true);
         const char *p5 = getenv("S2DW_PFA511");
         set_pfa511(p5 ? atoi(p5) != 0 : true);
+        const char *ps = getenv("S2DW_PFA_SMALL");
+        set_pfa_small(ps ? atoi(ps) != 0 : true);
     }
     {
         const char *ap = getenv("S2DW_ALPHA_PREFETCH");
