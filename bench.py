@@ -50,8 +50,8 @@ UNIT = "pairs/s"
 # analysis+synthesis pair at B=1024 N=4 alpha=2 J=10, from the ncu launch list
 # of `python -m s2dw_b200.workload 1024 4 1` (profiles/launches_B1024_N4.md).
 # Used only for the roofline "traffic" entry of that workload.
-NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.33e6, "mwalk": 10.80e6, "ana_beta": 27.19e6,
-                                "ana_alpha": 44.41e6, "syn_alpha": 44.31e6, "syn_beta": 30.98e6}}
+NCU_TRAFFIC = {(1024, 4, 2.0): {"lwalk": 7.18e6, "mwalk": 10.89e6, "ana_beta": 27.22e6,
+                                "ana_alpha": 44.23e6, "syn_alpha": 44.30e6, "syn_beta": 31.00e6}}
 NCU_TRAFFIC_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
                       "--clock-control none of `python -m s2dw_b200.workload 1024 4 1` (one pair, 11 launches of "
                       "each kind), profiles/launches_B1024_N4.md")
